@@ -1,0 +1,159 @@
+"""ctypes mirror of include/clothcraft.h (structure layouts only).
+
+Kept free of any library loading so that both the CUDA library binding and
+test tooling can share one definition of the C structures.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+CC_OK = 0
+CC_ERR_INVALID_ARGUMENT = 1
+CC_ERR_INVALID_STATE = 2
+CC_ERR_CONTACT = 3
+CC_ERR_NON_FINITE = 4
+CC_ERR_CAPACITY = 5
+CC_ERR_CUDA = 6
+CC_ERR_DEVICE_TIMEOUT = 7
+
+KIND_NAMES = ("PointPoint", "PointEdge", "PointFace", "EdgeEdge")
+
+c_double_p = C.POINTER(C.c_double)
+c_uint32_p = C.POINTER(C.c_uint32)
+c_uint8_p = C.POINTER(C.c_uint8)
+c_uint64_p = C.POINTER(C.c_uint64)
+
+
+class cc_material(C.Structure):
+    _fields_ = [(name, C.c_double) for name in (
+        "warp", "weft", "shear", "compression_ratio", "compression_transition",
+        "bend_warp", "bend_weft", "density", "thickness", "grain_degrees")]
+
+
+class cc_mesh(C.Structure):
+    _fields_ = [
+        ("n_vertices", C.c_uint64),
+        ("n_triangles", C.c_uint64),
+        ("triangles", c_uint32_p),
+        ("inv_dm", c_double_p),
+        ("area", c_double_p),
+        ("triangle_material", c_uint32_p),
+        ("n_hinges", C.c_uint64),
+        ("hinges", c_uint32_p),
+        ("hinge_weight", c_double_p),
+        ("hinge_across", c_double_p),
+        ("hinge_material", c_uint32_p),
+        ("n_materials", C.c_uint64),
+        ("materials", C.POINTER(cc_material)),
+        ("masses", c_double_p),
+        ("pinned", c_uint8_p),
+        ("pin_positions", c_double_p),
+        ("n_stitches", C.c_uint64),
+        ("stitch_offsets", c_uint32_p),
+        ("stitch_vertices", c_uint32_p),
+        ("stitch_weights", c_double_p),
+        ("stitch_stiffness", c_double_p),
+    ]
+
+
+class cc_surface(C.Structure):
+    _fields_ = [
+        ("n_vertices", C.c_uint64),
+        ("vertices", c_double_p),
+        ("n_triangles", C.c_uint64),
+        ("triangles", c_uint32_p),
+    ]
+
+
+class cc_ogc_settings(C.Structure):
+    _fields_ = [("radius", C.c_double), ("stiffness", C.c_double),
+                ("relaxation", C.c_double), ("refresh_fraction", C.c_double)]
+
+
+class cc_vbd_settings(C.Structure):
+    _fields_ = [
+        ("dt", C.c_double),
+        ("iterations", C.c_uint32),
+        ("reserved0", C.c_uint32),
+        ("damping", C.c_double),
+        ("gravity", C.c_double * 3),
+        ("contact", cc_ogc_settings),
+    ]
+
+
+class cc_grab(C.Structure):
+    _fields_ = [
+        ("vertices", C.c_uint32 * 3),
+        ("reserved0", C.c_uint32),
+        ("weights", C.c_double * 3),
+        ("target", C.c_double * 3),
+        ("stiffness", C.c_double),
+    ]
+
+
+class cc_metrics(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "time_s", "dt_s", "step_ms", "detection_ms", "solve_ms", "gpu_compute_ms",
+        "refit_ms", "candidates_ms", "narrow_ms")] + [(n, C.c_uint64) for n in (
+            "candidate_pairs", "aabb_rejections", "iterations", "contacts", "contact_terms",
+            "detection_updates", "broad_phase_rebuilds", "truncated_vertices", "colors")] + [
+        (n, C.c_double) for n in (
+            "minimum_distance_m", "max_seam_gap_m", "extension_p95_percent",
+            "extension_max_percent", "residual_rms_n")] + [
+        ("has_residual", C.c_int32), ("reserved0", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
+        d["residual_rms_n"] = d["residual_rms_n"] if d.pop("has_residual") else None
+        return d
+
+
+class cc_contacts(C.Structure):
+    _fields_ = [
+        ("contact_capacity", C.c_uint64),
+        ("incident_capacity", C.c_uint64),
+        ("radii_capacity", C.c_uint64),
+        ("kinds", c_uint8_p),
+        ("vertices", c_uint32_p),
+        ("counts", c_uint8_p),
+        ("mollifier_epsilon", c_double_p),
+        ("incident_offsets", c_uint64_p),
+        ("incident", c_uint32_p),
+        ("radii", c_double_p),
+        ("n_contacts", C.c_uint64),
+        ("n_incident", C.c_uint64),
+        ("active_contacts", C.c_uint64),
+        ("vertex_face_candidates", C.c_uint64),
+        ("edge_edge_candidates", C.c_uint64),
+        ("candidate_pairs", C.c_uint64),
+        ("aabb_rejections", C.c_uint64),
+        ("minimum_distance", C.c_double),
+        ("broad_phase_rebuilt", C.c_int32),
+        ("reserved0", C.c_int32),
+    ]
+
+
+class cc_candidates(C.Structure):
+    _fields_ = [
+        ("vf_capacity", C.c_uint64), ("ee_capacity", C.c_uint64),
+        ("vf", c_uint32_p), ("ee", c_uint32_p),
+        ("n_vf", C.c_uint64), ("n_ee", C.c_uint64),
+    ]
+
+
+def ptr(a: np.ndarray | None, ctype):
+    """Pointer to a contiguous numpy array (or NULL)."""
+    if a is None:
+        return C.cast(None, C.POINTER(ctype))
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def as_f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def as_u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)

@@ -1,0 +1,255 @@
+/*
+ * clothcraft.h — C ABI of the B200-native ClothCraft physics step.
+ *
+ * The library replaces the hybrid wgpu backend of ClothCraft with a CUDA
+ * (sm_100a) implementation of the whole step: Vertex Block Descent colour
+ * sweeps plus the Offset Geometric Contact (OGC) pipeline, both resident on
+ * one GPU. Each entry point names the reference interface it stands in for
+ * (paths are inside the ClothCraft source tree).
+ *
+ * Conventions (mirroring the reference's Rust surface):
+ *   - SI units, f64 in and out. Positions and velocities are n x 3 row-major
+ *     doubles (the memory image of Vec<DVec3>).
+ *   - Every fallible call returns an int32 status (CC_OK on success) and is
+ *     transactional: caller arrays are written only on CC_OK
+ *     (src/vbd.rs:249,399-405; tests/vbd.rs:88-90).
+ *   - The message of the last failure on a handle is read with cc_last_error;
+ *     failures without a handle (creation) with cc_global_last_error.
+ *   - One handle is driven by one host thread at a time, as GpuVbd is
+ *     (RefCell, src/gpu_vbd.rs:15-25). The library owns all device memory.
+ *   - Index arrays are uint32. No torch or CUDA types cross this boundary.
+ */
+#ifndef CLOTHCRAFT_H
+#define CLOTHCRAFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CC_ABI_VERSION 1
+
+enum cc_status {
+    CC_OK = 0,
+    CC_ERR_INVALID_ARGUMENT = 1, /* settings, dimensions, indices          */
+    CC_ERR_INVALID_STATE = 2,    /* non-finite state, moved fixed geometry */
+    CC_ERR_CONTACT = 3,          /* zero separation, initial intersection, */
+                                 /* trust-region invariant                 */
+    CC_ERR_NON_FINITE = 4,       /* non-finite result, state unchanged     */
+    CC_ERR_CAPACITY = 5,         /* caller buffer too small; sizes written */
+    CC_ERR_CUDA = 6,             /* CUDA runtime failure                   */
+    CC_ERR_DEVICE_TIMEOUT = 7    /* a bounded device wait gave up          */
+};
+
+/* Material (src/model.rs:7-22). grain_degrees rotates the fibre frame. */
+typedef struct cc_material {
+    double warp, weft, shear;
+    double compression_ratio, compression_transition;
+    double bend_warp, bend_weft;
+    double density, thickness, grain_degrees;
+} cc_material;
+
+/* The cloth: Mesh (src/model.rs:91-115) plus the seam stitch terms that
+ * VbdSolver::new flattens (src/vbd.rs:128-144, src/garment/seam.rs:215-238).
+ * Stitch s covers stitch_vertices/weights[stitch_offsets[s] ..
+ * stitch_offsets[s+1]) and has stiffness seam.stiffness * weight_m. */
+typedef struct cc_mesh {
+    uint64_t n_vertices;
+    uint64_t n_triangles;
+    const uint32_t* triangles;         /* [n_triangles][3]                     */
+    const double* inv_dm;              /* [n_triangles][4]: x_axis.xy, y_axis.xy */
+    const double* area;                /* [n_triangles]                        */
+    const uint32_t* triangle_material; /* [n_triangles]                        */
+    uint64_t n_hinges;
+    const uint32_t* hinges;            /* [n_hinges][4]: shared edge a,b; c; d */
+    const double* hinge_weight;        /* [n_hinges]                           */
+    const double* hinge_across;        /* [n_hinges][2]                        */
+    const uint32_t* hinge_material;    /* [n_hinges]                           */
+    uint64_t n_materials;
+    const cc_material* materials;      /* [n_materials]                        */
+    const double* masses;              /* [n_vertices]                         */
+    const uint8_t* pinned;             /* [n_vertices], 1 = pinned             */
+    const double* pin_positions;       /* [n_vertices][3], read where pinned   */
+    uint64_t n_stitches;
+    const uint32_t* stitch_offsets;    /* [n_stitches + 1]                     */
+    const uint32_t* stitch_vertices;   /* [stitch_offsets[n_stitches]]         */
+    const double* stitch_weights;      /* [stitch_offsets[n_stitches]]         */
+    const double* stitch_stiffness;    /* [n_stitches]                         */
+} cc_mesh;
+
+/* Fixed obstacle: SurfaceMesh (src/avatar.rs:8-11). */
+typedef struct cc_surface {
+    uint64_t n_vertices;
+    const double* vertices;            /* [n_vertices][3] */
+    uint64_t n_triangles;
+    const uint32_t* triangles;         /* [n_triangles][3] */
+} cc_surface;
+
+/* OgcSettings (src/ogc/world.rs:33-71). */
+typedef struct cc_ogc_settings {
+    double radius;
+    double stiffness;
+    double relaxation;
+    double refresh_fraction;
+} cc_ogc_settings;
+
+/* VbdSettings (src/vbd.rs:18-52). */
+typedef struct cc_vbd_settings {
+    double dt;
+    uint32_t iterations;
+    uint32_t reserved0;
+    double damping;
+    double gravity[3];
+    cc_ogc_settings contact;
+} cc_vbd_settings;
+
+/* Grab (src/vbd.rs:54-60): mouse attachment, weights sum to one. */
+typedef struct cc_grab {
+    uint32_t vertices[3];
+    uint32_t reserved0;
+    double weights[3];
+    double target[3];
+    double stiffness;
+} cc_grab;
+
+/* VbdMetrics (src/vbd.rs:61-83) with DetectionProfile (src/ogc/world.rs:14-22). */
+typedef struct cc_metrics {
+    double time_s, dt_s, step_ms, detection_ms, solve_ms;
+    double gpu_compute_ms;          /* device time of the step, CUDA events   */
+    double refit_ms, candidates_ms, narrow_ms;
+    uint64_t candidate_pairs, aabb_rejections;
+    uint64_t iterations, contacts, contact_terms;
+    uint64_t detection_updates, broad_phase_rebuilds, truncated_vertices;
+    uint64_t colors;                /* colours of the last sweep              */
+    double minimum_distance_m, max_seam_gap_m;
+    double extension_p95_percent, extension_max_percent;
+    double residual_rms_n;
+    int32_t has_residual;           /* 1 when residual_rms_n is defined       */
+    int32_t reserved0;
+} cc_metrics;
+
+/* ContactSet (src/ogc/world.rs:73-107) in caller-owned arrays. The contact
+ * list is in canonical order: sorted by (kind, vertices), deduplicated. If a
+ * capacity is too small the call returns CC_ERR_CAPACITY and fills the
+ * n_contacts / n_incident / n_vf_pairs / n_ee_pairs it needs. */
+typedef struct cc_contacts {
+    /* capacities (in) */
+    uint64_t contact_capacity;
+    uint64_t incident_capacity;
+    uint64_t radii_capacity;          /* >= number of moving vertices */
+    /* arrays (out; may be NULL when the matching capacity is 0) */
+    uint8_t* kinds;                   /* 0 PointPoint, 1 PointEdge, 2 PointFace, 3 EdgeEdge */
+    uint32_t* vertices;               /* [contact][4] */
+    uint8_t* counts;
+    double* mollifier_epsilon;
+    uint64_t* incident_offsets;       /* [moving + 1] */
+    uint32_t* incident;               /* contact ids per moving vertex, ascending */
+    double* radii;                    /* [moving] */
+    /* scalars (out) */
+    uint64_t n_contacts;
+    uint64_t n_incident;
+    uint64_t active_contacts;
+    uint64_t vertex_face_candidates;
+    uint64_t edge_edge_candidates;
+    uint64_t candidate_pairs;
+    uint64_t aabb_rejections;
+    double minimum_distance;
+    int32_t broad_phase_rebuilt;
+    int32_t reserved0;
+} cc_contacts;
+
+/* Candidate pairs of a fresh broad phase (Candidates::build,
+ * src/ogc/candidates.rs:23-68), sorted ascending, for list parity tests. */
+typedef struct cc_candidates {
+    uint64_t vf_capacity, ee_capacity;
+    uint32_t* vf;                     /* [pair][2]: point, triangle */
+    uint32_t* ee;                     /* [pair][2]: edge, edge (operand order of the reference) */
+    uint64_t n_vf, n_ee;
+} cc_candidates;
+
+typedef struct cc_solver cc_solver;
+typedef struct cc_world cc_world;
+
+/* ---------------------------------------------------------------- library */
+int32_t cc_abi_version(void);
+/* Message of the last failure that had no handle (creation). */
+int32_t cc_global_last_error(char* buffer, uint64_t length);
+/* Message of the last failure on a handle; returns its status. */
+int32_t cc_last_error(const cc_solver* solver, char* buffer, uint64_t length);
+int32_t cc_world_last_error(const cc_world* world, char* buffer, uint64_t length);
+/* Device the library runs on (default 0); call before creating handles. */
+int32_t cc_set_device(int32_t device);
+
+/* ----------------------------------------------------------------- solver */
+/* VbdSolver::new (src/vbd.rs:101-192): checks dimensions and pins, appends
+ * the obstacle, builds stitches and exclusions, OgcWorld::new and
+ * validate_start, incidence and the material graph. x0/v0: [n][3]. */
+int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle,
+                         const double* x0, const double* v0, uint64_t n,
+                         cc_solver** out);
+void cc_solver_destroy(cc_solver* solver);
+
+/* VbdSolver::step (src/vbd.rs:250-422) with GpuVbd::step's slot
+ * (src/gpu_vbd.rs:125-131): x, v ([n][3]) and *time are read, and written
+ * only on CC_OK. grab may be NULL. metrics may be NULL. */
+int32_t cc_solver_step(cc_solver* solver, double* x, double* v, double* time,
+                       const cc_vbd_settings* settings, const cc_grab* grab,
+                       cc_metrics* metrics);
+
+/* Device-resident stepping: the state stays in HBM between calls.
+ * set_state uploads x, v, time; step_resident advances it; get_state reads
+ * it back. Same semantics as cc_solver_step otherwise. */
+int32_t cc_solver_set_state(cc_solver* solver, const double* x, const double* v, double time);
+int32_t cc_solver_get_state(cc_solver* solver, double* x, double* v, double* time);
+int32_t cc_solver_step_resident(cc_solver* solver, const cc_vbd_settings* settings,
+                                const cc_grab* grab, cc_metrics* metrics);
+
+/* Number of cloth (moving) vertices and of all vertices including the obstacle. */
+uint64_t cc_solver_moving(const cc_solver* solver);
+uint64_t cc_solver_total(const cc_solver* solver);
+
+/* The solver's OGC world (owned by the solver; do not destroy). */
+cc_world* cc_solver_world(cc_solver* solver);
+
+/* Colouring (coloring::colors, src/vbd/coloring.rs:5-43) of the material
+ * graph plus a contact set detected at x_all, plus an optional grab.
+ * colors_out: [moving] colour per vertex; *n_colors: number of colours. */
+int32_t cc_solver_colors(cc_solver* solver, const double* x_all, double query_radius,
+                         const cc_ogc_settings* settings, const cc_grab* grab,
+                         uint32_t* colors_out, uint32_t* n_colors);
+
+/* Local block of every moving vertex at positions x_all with the contact set
+ * detected at x_all (VbdSolver::local with Jet<3>, src/vbd.rs:196-248, plus
+ * the inertia of the step, src/vbd.rs:353-356; the GPU probe of
+ * src/vbd.wgsl:142-147). targets/inertia: [moving][3] / [moving] or NULL for
+ * no inertia. energy [moving], gradient [moving][3], hessian [moving][9]. */
+int32_t cc_solver_local_blocks(cc_solver* solver, const double* x_all,
+                               double query_radius, const cc_vbd_settings* settings,
+                               const cc_grab* grab, const double* targets,
+                               const double* inertia, double* energy,
+                               double* gradient, double* hessian);
+
+/* ------------------------------------------------------------------ world */
+/* OgcWorld::new (src/ogc/world.rs:126-211). x: [n_all][3]; vertices >= moving
+ * are fixed. excluded: [n_excluded][2] vertex pairs never in contact. */
+int32_t cc_world_create(const double* x, uint64_t n_all, const uint32_t* triangles,
+                        uint64_t n_triangles, uint64_t moving,
+                        const uint32_t* excluded, uint64_t n_excluded, cc_world** out);
+void cc_world_destroy(cc_world* world);
+/* OgcWorld::validate_start (src/ogc/world.rs:242-307). */
+int32_t cc_world_validate_start(cc_world* world, const double* x);
+/* OgcWorld::detect (src/ogc/world.rs:308-420), candidate cache included. */
+int32_t cc_world_detect(cc_world* world, const double* x, double query_radius,
+                        const cc_ogc_settings* settings, cc_contacts* out);
+/* Fresh broad phase at search radius `radius` (no cache), sorted lists. */
+int32_t cc_world_candidates(cc_world* world, const double* x, double radius,
+                            cc_candidates* out);
+/* Topology sizes: edges of the combined mesh (src/ogc/topology.rs:13-52). */
+uint64_t cc_world_edges(const cc_world* world, uint32_t* edges_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLOTHCRAFT_H */

@@ -1,0 +1,344 @@
+// Oracle (test infrastructure only): FP64 restatement of ClothCraft's CPU VBD
+// step (src/vbd.rs:101-422) and its helpers.
+#include "oracle_vbd.hpp"
+
+#include <chrono>
+#include <cstdio>
+
+namespace oracle {
+
+static double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+bool VbdSettings::valid() const {  // src/vbd.rs:38-51
+    if (!contact.valid()) return false;
+    return std::isfinite(dt) && dt >= 1e-6 && dt <= 0.025 && iterations != 0 && iterations <= 200 &&
+           std::isfinite(damping) && damping >= 0.0 && finite(gravity);
+}
+
+// src/vbd/prediction.rs:15-41
+std::vector<D3> Prediction::guess(const State& state, const VbdSettings& s) const {
+    bool valid = false;
+    if (has_last) {
+        valid = last.time == state.time && last.x.size() == state.x.size() && last.v.size() == state.v.size() &&
+                gravity == s.gravity && damping == s.damping;
+        for (size_t i = 0; valid && i < state.x.size(); ++i) valid = last.x[i] == state.x[i];
+        for (size_t i = 0; valid && i < state.v.size(); ++i) valid = last.v[i] == state.v[i];
+    }
+    double g2 = length_squared(s.gravity);
+    std::vector<D3> out(state.x.size());
+    for (size_t i = 0; i < state.x.size(); ++i) {
+        double factor = 1.0;
+        if (valid && g2 > 1e-20) {
+            double f = dot(acceleration[i], s.gravity) / g2;
+            factor = f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
+        }
+        out[i] = state.x[i] + (state.v[i] * s.dt + s.gravity * factor * (s.dt * s.dt)) / (1.0 + s.damping * s.dt);
+    }
+    return out;
+}
+
+// src/vbd/prediction.rs:43-54
+void Prediction::record(const std::vector<D3>& old_velocity, const State& state, const VbdSettings& s) {
+    acceleration.resize(state.v.size());
+    for (size_t i = 0; i < state.v.size(); ++i)
+        acceleration[i] = (state.v[i] - old_velocity[i]) / s.dt + state.v[i] * s.damping;
+    last = state;
+    has_last = true;
+    gravity = s.gravity;
+    damping = s.damping;
+}
+
+// src/vbd/coloring.rs:5-43
+std::vector<std::vector<uint32_t>> greedy_colors(const std::vector<std::vector<uint32_t>>& graph,
+                                                 const ContactSet& contact, const Grab* grab) {
+    const size_t n = graph.size();
+    const size_t none = (size_t)-1;
+    std::vector<size_t> assigned(n, none);
+    std::vector<std::vector<uint32_t>> colors;
+    std::vector<size_t> seen(n + 1, none);
+    for (size_t v = 0; v < n; ++v) {
+        auto mark = [&](size_t i) {
+            if (i < n && assigned[i] != none) seen[assigned[i]] = v;
+        };
+        for (uint32_t i : graph[v]) mark(i);
+        for (uint32_t idx : contact.incident[v]) {
+            const Contact& c = contact.contacts[idx];
+            for (int k = 0; k < c.count; ++k) mark(c.vertices[k]);
+        }
+        if (grab && grab->contains((uint32_t)v))
+            for (uint32_t i : grab->vertices) mark(i);
+        size_t c = 0;
+        while (seen[c] == v) ++c;
+        if (c == colors.size()) colors.emplace_back();
+        colors[c].push_back((uint32_t)v);
+        assigned[v] = c;
+    }
+    return colors;
+}
+
+// src/garment/diagnostics.rs:7-27 with energy::fiber_frame stretches (src/energy.rs:93-114)
+std::array<double, 2> extension_percent(const Mesh& mesh, const std::vector<D3>& x) {
+    std::vector<std::pair<double, double>> values;
+    values.reserve(mesh.triangles.size());
+    for (const Triangle& t : mesh.triangles) {
+        const Material& m = mesh.materials[t.material];
+        D3 ds0 = x[t.vertices[1]] - x[t.vertices[0]];
+        D3 ds1 = x[t.vertices[2]] - x[t.vertices[0]];
+        D3 f0 = ds0 * t.inv_dm[0] + ds1 * t.inv_dm[1];
+        D3 f1 = ds0 * t.inv_dm[2] + ds1 * t.inv_dm[3];
+        double s, c;
+        grain_sin_cos(m.grain_degrees, s, c);
+        D3 w = f0 * c + f1 * s;
+        D3 v = -f0 * s + f1 * c;
+        double stretch = std::fmax(length(w), length(v));
+        values.push_back({100.0 * std::fmax(stretch - 1.0, 0.0), t.area});
+    }
+    std::sort(values.begin(), values.end(), [](auto& a, auto& b) { return a.first < b.first; });
+    double total = 0.0;
+    for (auto& v : values) total += v.second;
+    double area = 0.0, p95 = 0.0;
+    for (auto& v : values) {
+        area += v.second;
+        if (area >= 0.95 * total) {
+            p95 = v.first;
+            break;
+        }
+    }
+    return {p95, values.empty() ? 0.0 : values.back().first};
+}
+
+// src/vbd.rs:101-192
+VbdSolver VbdSolver::make(const Mesh& mesh, const std::vector<D3>* obstacle_x,
+                          const std::vector<std::array<uint32_t, 3>>* obstacle_tris, const State& state) {
+    const size_t n = mesh.n;
+    if (state.x.size() != n || state.v.size() != n) throw Error{1, "VBD state dimensions do not match garment"};
+    for (size_t i = 0; i < n; ++i)
+        if (mesh.pinned[i] && distance(state.x[i], mesh.pin_positions[i]) > 1e-10)
+            throw Error{1, "VBD pinned positions must match their constraints before initialization"};
+    std::vector<D3> x = state.x;
+    std::vector<std::array<uint32_t, 3>> faces;
+    for (const auto& t : mesh.triangles) faces.push_back(t.vertices);
+    if (obstacle_x) {
+        if (obstacle_x->empty() || obstacle_tris->empty()) throw Error{1, "Empty/non-finite avatar"};
+        for (const auto& p : *obstacle_x)
+            if (!finite(p)) throw Error{1, "Empty/non-finite avatar"};
+        for (const auto& t : *obstacle_tris) {  // src/avatar.rs:88-97
+            if (t[0] >= obstacle_x->size() || t[1] >= obstacle_x->size() || t[2] >= obstacle_x->size())
+                throw Error{1, "Invalid avatar index"};
+            D3 a = (*obstacle_x)[t[0]], b = (*obstacle_x)[t[1]], c = (*obstacle_x)[t[2]];
+            if (length_squared(cross(b - a, c - a)) < 1e-24) throw Error{1, "Degenerate avatar triangle"};
+        }
+        x.insert(x.end(), obstacle_x->begin(), obstacle_x->end());
+        for (const auto& t : *obstacle_tris)
+            faces.push_back({t[0] + (uint32_t)n, t[1] + (uint32_t)n, t[2] + (uint32_t)n});
+    }
+    std::vector<std::array<uint32_t, 2>> excluded;
+    for (const Stitch& s : mesh.stitches)
+        for (const auto& [a, wa] : s.terms)
+            for (const auto& [b, wb] : s.terms)
+                if (wa * wb < 0.0) excluded.push_back({std::min(a, b), std::max(a, b)});
+    VbdSolver solver;
+    solver.mesh = mesh;
+    solver.world = OgcWorld::make(x, faces, n, excluded);
+    solver.world.validate_start(x);
+    solver.triangles.assign(n, {});
+    solver.hinges.assign(n, {});
+    solver.vertex_stitches.assign(n, {});
+    std::vector<std::set<uint32_t>> graph(n);
+    auto connect = [&](const uint32_t* ids, size_t count) {
+        for (size_t a = 0; a < count; ++a)
+            for (size_t b = 0; b < count; ++b)
+                if (ids[a] != ids[b]) graph[ids[a]].insert(ids[b]);
+    };
+    for (size_t i = 0; i < mesh.triangles.size(); ++i) {
+        for (uint32_t v : mesh.triangles[i].vertices) solver.triangles[v].push_back((uint32_t)i);
+        connect(mesh.triangles[i].vertices.data(), 3);
+    }
+    for (size_t i = 0; i < mesh.hinges.size(); ++i) {
+        for (uint32_t v : mesh.hinges[i].vertices) solver.hinges[v].push_back((uint32_t)i);
+        connect(mesh.hinges[i].vertices.data(), 4);
+    }
+    for (size_t i = 0; i < mesh.stitches.size(); ++i) {
+        std::vector<uint32_t> ids;
+        for (const auto& t : mesh.stitches[i].terms) ids.push_back(t.first);
+        for (uint32_t v : ids) solver.vertex_stitches[v].push_back((uint32_t)i);
+        connect(ids.data(), ids.size());
+    }
+    solver.graph.resize(n);
+    for (size_t i = 0; i < n; ++i) solver.graph[i].assign(graph[i].begin(), graph[i].end());
+    return solver;
+}
+
+std::vector<std::vector<uint32_t>> VbdSolver::colors(const ContactSet& contact, const Grab* grab) const {
+    return greedy_colors(graph, contact, grab);
+}
+
+namespace {
+struct Update {
+    uint32_t v;
+    D3 p;
+    bool truncated;
+    double residual;
+};
+}  // namespace
+
+// src/vbd.rs:250-422
+VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab* grab) {
+    if (!settings.valid()) throw Error{1, "Invalid VBD settings"};
+    const size_t n = mesh.n;
+    bool ok = state.x.size() == n && state.v.size() == n && std::isfinite(state.time);
+    for (size_t i = 0; ok && i < n; ++i) ok = finite(state.x[i]) && finite(state.v[i]);
+    if (!ok) throw Error{2, "Invalid VBD state"};
+    if (grab) {
+        double sum = grab->weights[0] + grab->weights[1] + grab->weights[2];
+        bool bad = !finite(grab->target) || !std::isfinite(grab->stiffness) || grab->stiffness <= 0.0 ||
+                   std::fabs(sum - 1.0) > 1e-8;
+        for (int i = 0; i < 3; ++i)
+            bad = bad || grab->vertices[i] >= n || !std::isfinite(grab->weights[i]) || grab->weights[i] < 0.0;
+        if (bad) throw Error{1, "Invalid mouse attachment"};
+    }
+    double start = now_ms();
+    VbdMetrics metrics;
+    metrics.dt_s = settings.dt;
+    metrics.iterations = settings.iterations;
+    const double dt = settings.dt;
+    std::vector<D3> old_velocity = state.v;
+    std::vector<D3> guess = prediction.guess(state, settings);
+    const double damp = 1.0 + settings.damping * dt;
+    std::vector<D3> target(n);
+    std::vector<double> inertia(n);
+    double predicted_motion = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        target[i] = state.x[i] + (state.v[i] * dt + settings.gravity * dt * dt) / damp;
+        inertia[i] = mesh.masses[i] * damp / (dt * dt);
+        predicted_motion = std::fmax(predicted_motion, distance(target[i], state.x[i]));
+    }
+    double r = settings.contact.radius;
+    double rq = std::min(std::max(r + predicted_motion, 2.0 * r), 4.0 * r);  // f64::clamp
+    std::vector<D3> x = world.positions(state.x.data(), n);
+    double t_detect = now_ms();
+    ContactSet contacts = world.detect(x, rq, settings.contact);
+    if (contacts.minimum_distance <= 1e-12)
+        throw Error{3, "OGC zero separation; step rejected, reset the arrangement"};
+    metrics.detection_ms += now_ms() - t_detect;
+    metrics.detection_updates += 1;
+    metrics.broad_phase_rebuilds += contacts.broad_phase_rebuilt ? 1 : 0;
+    auto add_profile = [&](const DetectionProfile& p) {
+        metrics.profile.refit_ms += p.refit_ms;
+        metrics.profile.candidates_ms += p.candidates_ms;
+        metrics.profile.narrow_ms += p.narrow_ms;
+        metrics.profile.candidate_pairs += p.candidate_pairs;
+        metrics.profile.aabb_rejections += p.aabb_rejections;
+    };
+    add_profile(contacts.profile);
+    std::vector<std::vector<uint32_t>> colors = this->colors(contacts, grab);
+    size_t clipped = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (!mesh.pinned[i]) {
+            bool b;
+            x[i] = contacts.truncate(i, guess[i], b);
+            clipped += b ? 1 : 0;
+        }
+    }
+    std::vector<Update> updates;
+    for (size_t it = 0; it < settings.iterations; ++it) {
+        if (clipped > 0 && (double)clipped >= settings.contact.refresh_fraction * (double)n) {
+            double t = now_ms();
+            contacts = world.detect(x, rq, settings.contact);
+            colors = this->colors(contacts, grab);
+            metrics.detection_ms += now_ms() - t;
+            metrics.detection_updates += 1;
+            metrics.broad_phase_rebuilds += contacts.broad_phase_rebuilt ? 1 : 0;
+            add_profile(contacts.profile);
+        }
+        clipped = 0;
+        double residual = 0.0;
+        for (const auto& color : colors) {
+            updates.resize(color.size());
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 64)
+            for (size_t ci = 0; ci < color.size(); ++ci) {
+                uint32_t v = color[ci];
+                if (mesh.pinned[v]) {
+                    updates[ci] = {v, x[v], false, 0.0};
+                    continue;
+                }
+                V3<Jet<3>> p;
+                for (int k = 0; k < 3; ++k) p[k] = variable<3>(x[v][k], k);
+                Jet<3> jet = local<Jet<3>>(v, p, x, contacts, settings, grab);
+                D3 g = D3{jet.g[0], jet.g[1], jet.g[2]} + (x[v] - target[v]) * inertia[v];
+                M3 h;
+                for (int col = 0; col < 3; ++col) h.c[col] = {jet.h[0][col], jet.h[1][col], jet.h[2][col]};
+                h = h + m3_identity_scaled(inertia[v]);
+                double lower = std::numeric_limits<double>::infinity();
+                for (int i = 0; i < 3; ++i) {
+                    double sum = 0.0;
+                    for (int j = 0; j < 3; ++j)
+                        if (j != i) sum += std::fabs(h.c[i][j]);
+                    lower = std::fmin(lower, h.c[i][i] - sum);
+                }
+                if (lower < 1e-8) h = h + m3_identity_scaled(1e-8 - lower + 0.01 * inertia[v]);
+                D3 delta = -mul(inverse(h), g);
+                double old = jet.v + 0.5 * inertia[v] * length_squared(x[v] - target[v]);
+                D3 accepted = x[v];
+                bool truncated = false;
+                double scale = 1.0;
+                for (int attempt = 0; attempt < 10; ++attempt) {
+                    D3 candidate = x[v] + delta * scale;  // 0.5_f64.powi(attempt) is exact
+                    scale *= 0.5;
+                    bool bound;
+                    candidate = contacts.truncate(v, candidate, bound);
+                    truncated = truncated || bound;
+                    double e = local<double>(v, lift<double>(candidate), x, contacts, settings, grab) +
+                               0.5 * inertia[v] * length_squared(candidate - target[v]);
+                    if (finite(candidate) && std::isfinite(e) && e <= old + 1e-14) {
+                        accepted = candidate;
+                        break;
+                    }
+                }
+                updates[ci] = {v, accepted, truncated, length_squared(g)};
+            }
+            for (const Update& u : updates) {
+                x[u.v] = u.p;
+                clipped += u.truncated ? 1 : 0;
+                residual += u.residual;
+            }
+        }
+        metrics.truncated_vertices += clipped;
+        metrics.residual_rms_n = std::sqrt(residual / (double)(3 * n));
+        metrics.has_residual = true;
+        metrics.colors = colors.size();
+    }
+    for (const auto& p : x)
+        if (!finite(p)) throw Error{4, "Non-finite VBD result; state unchanged"};
+    for (size_t i = 0; i < n; ++i)
+        if (distance(x[i], contacts.centers[i]) > contacts.radii[i] + 1e-10)
+            throw Error{3, "OGC trust-region invariant failed"};
+    for (size_t i = 0; i < n; ++i) {
+        state.v[i] = (x[i] - state.x[i]) / dt;
+        state.x[i] = x[i];
+    }
+    state.time += dt;
+    prediction.record(old_velocity, state, settings);
+    metrics.time_s = state.time;
+    metrics.contacts = contacts.active_contacts;
+    metrics.contact_terms = contacts.contacts.size();
+    metrics.minimum_distance_m = contacts.minimum_distance;
+    double gap = 0.0;
+    for (const Stitch& s : mesh.stitches) {
+        D3 d{0, 0, 0};
+        for (const auto& [j, w] : s.terms) d = d + state.x[j] * w;
+        gap = std::fmax(gap, length(d));
+    }
+    metrics.max_seam_gap_m = gap;
+    auto ext = extension_percent(mesh, state.x);
+    metrics.extension_p95_percent = ext[0];
+    metrics.extension_max_percent = ext[1];
+    metrics.step_ms = now_ms() - start;
+    metrics.solve_ms = metrics.step_ms - metrics.detection_ms;
+    return metrics;
+}
+
+}  // namespace oracle
