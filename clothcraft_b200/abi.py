@@ -102,7 +102,9 @@ class cc_metrics(C.Structure):
         (n, C.c_double) for n in (
             "minimum_distance_m", "max_seam_gap_m", "extension_p95_percent",
             "extension_max_percent", "residual_rms_n")] + [
-        ("has_residual", C.c_int32), ("reserved0", C.c_int32)]
+        ("has_residual", C.c_int32), ("reserved0", C.c_int32),
+        ("sweep_ms", C.c_double)] + [(n, C.c_uint64) for n in (
+            "sweep_launches", "vertex_solves", "kernel_launches", "contact_incidence")]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
@@ -157,3 +159,46 @@ def as_f64(a) -> np.ndarray:
 
 def as_u32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+class ContactResult(dict):
+    """ContactSet fields as numpy arrays / scalars."""
+
+
+def read_contacts(call, moving: int, contact_hint: int = 4096) -> ContactResult:
+    """Two-call protocol around a cc_contacts-filling function."""
+    cap = contact_hint
+    while True:
+        out = cc_contacts()
+        kinds = np.zeros(cap, np.uint8)
+        verts = np.zeros((cap, 4), np.uint32)
+        counts = np.zeros(cap, np.uint8)
+        eps = np.zeros(cap)
+        inc_off = np.zeros(moving + 1, np.uint64)
+        inc = np.zeros(4 * cap, np.uint32)
+        radii = np.zeros(max(moving, 1))
+        out.contact_capacity = cap
+        out.incident_capacity = 4 * cap
+        out.radii_capacity = moving
+        out.kinds = ptr(kinds, C.c_uint8)
+        out.vertices = ptr(verts, C.c_uint32)
+        out.counts = ptr(counts, C.c_uint8)
+        out.mollifier_epsilon = ptr(eps, C.c_double)
+        out.incident_offsets = ptr(inc_off, C.c_uint64)
+        out.incident = ptr(inc, C.c_uint32)
+        out.radii = ptr(radii, C.c_double)
+        rc = call(out)
+        if rc == CC_ERR_CAPACITY:
+            cap = max(int(out.n_contacts), int(out.n_incident) // 4 + 1, 2 * cap)
+            continue
+        if rc != CC_OK:
+            return rc
+        k = int(out.n_contacts)
+        r = ContactResult(
+            kinds=kinds[:k].copy(), vertices=verts[:k].copy(), counts=counts[:k].copy(), epsilon=eps[:k].copy(),
+            incident_offsets=inc_off.copy(), incident=inc[:int(out.n_incident)].copy(), radii=radii[:moving].copy(),
+            active_contacts=int(out.active_contacts), vertex_face_candidates=int(out.vertex_face_candidates),
+            edge_edge_candidates=int(out.edge_edge_candidates), candidate_pairs=int(out.candidate_pairs),
+            aabb_rejections=int(out.aabb_rejections), minimum_distance=float(out.minimum_distance),
+            broad_phase_rebuilt=bool(out.broad_phase_rebuilt))
+        return r

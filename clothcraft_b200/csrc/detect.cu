@@ -1,0 +1,1301 @@
+// OGC detection on the device (replaces OgcWorld::detect, src/ogc/world.rs:308-557,
+// which the reference runs on the CPU every step).
+//
+// This translation unit is compiled with --fmad=false: every FP64 multiply and
+// add is rounded separately, as Rust's f64 arithmetic is, so that distances,
+// feasibility decisions, radii and contact keys are bit-identical to the CPU
+// path for identical positions.
+//
+// Pipeline per detection: primitive boxes -> candidate-cache coverage ->
+// (on a miss) Morton LBVH build + dual-tree-equivalent pair queries ->
+// FP64 narrow phase -> radix sort + dedup of contact keys -> incidence CSR ->
+// per-vertex minimum distance -> conservative radii.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <set>
+
+#include "world.cuh"
+
+namespace cc {
+
+// ------------------------------------------------------------------ boxes
+__device__ __forceinline__ void box_of3(d3 a, d3 b, d3 c, Box& o) {
+    // Bounds::points folds min/max from +inf/-inf (src/ogc/bvh.rs:9-20)
+    o.lo[0] = fmin(fmin(a.x, b.x), c.x);
+    o.lo[1] = fmin(fmin(a.y, b.y), c.y);
+    o.lo[2] = fmin(fmin(a.z, b.z), c.z);
+    o.hi[0] = fmax(fmax(a.x, b.x), c.x);
+    o.hi[1] = fmax(fmax(a.y, b.y), c.y);
+    o.hi[2] = fmax(fmax(a.z, b.z), c.z);
+}
+__device__ __forceinline__ void box_of2(d3 a, d3 b, Box& o) {
+    o.lo[0] = fmin(a.x, b.x);
+    o.lo[1] = fmin(a.y, b.y);
+    o.lo[2] = fmin(a.z, b.z);
+    o.hi[0] = fmax(a.x, b.x);
+    o.hi[1] = fmax(a.y, b.y);
+    o.hi[2] = fmax(a.z, b.z);
+}
+__device__ __forceinline__ void box_of1(d3 a, Box& o) {
+    o.lo[0] = o.hi[0] = a.x;
+    o.lo[1] = o.hi[1] = a.y;
+    o.lo[2] = o.hi[2] = a.z;
+}
+// Bounds::distance_squared (src/ogc/bvh.rs:31-36), same operation order.
+__device__ __forceinline__ double box_dist2(const Box& a, const Box& b) {
+    double dx = fmax(fmax(a.lo[0] - b.hi[0], b.lo[0] - a.hi[0]), 0.0);
+    double dy = fmax(fmax(a.lo[1] - b.hi[1], b.lo[1] - a.hi[1]), 0.0);
+    double dz = fmax(fmax(a.lo[2] - b.hi[2], b.lo[2] - a.hi[2]), 0.0);
+    return dx * dx + dy * dy + dz * dz;
+}
+// Bounds::overlaps (src/ogc/bvh.rs:27-29)
+__device__ __forceinline__ bool box_overlap(const Box& a, const Box& b) {
+    return a.lo[0] <= b.hi[0] && a.lo[1] <= b.hi[1] && a.lo[2] <= b.hi[2] && a.hi[0] >= b.lo[0] &&
+           a.hi[1] >= b.lo[1] && a.hi[2] >= b.lo[2];
+}
+__device__ __forceinline__ Box box_union(const Box& a, const Box& b) {
+    Box r;
+    for (int k = 0; k < 3; ++k) {
+        r.lo[k] = fmin(a.lo[k], b.lo[k]);
+        r.hi[k] = fmax(a.hi[k], b.hi[k]);
+    }
+    return r;
+}
+__device__ __forceinline__ Box ldcg_box(const Box* p) {
+    Box b;
+    const double* s = reinterpret_cast<const double*>(p);
+    b.lo[0] = __ldcg(s + 0);
+    b.lo[1] = __ldcg(s + 1);
+    b.lo[2] = __ldcg(s + 2);
+    b.hi[0] = __ldcg(s + 3);
+    b.hi[1] = __ldcg(s + 4);
+    b.hi[2] = __ldcg(s + 5);
+    return b;
+}
+
+// ------------------------------------------------------------------- LBVH
+__global__ void k_bounds_init(unsigned long long* b) {
+    if (threadIdx.x < 3) b[threadIdx.x] = ~0ull;
+    else if (threadIdx.x < 6) b[threadIdx.x] = 0ull;
+}
+
+__global__ void k_centroid_bounds(const Box* box, const uint32_t* ids, uint32_t m, unsigned long long* b) {
+    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        const Box& q = box[ids[i]];
+        for (int k = 0; k < 3; ++k) {
+            unsigned long long key = order_key(0.5 * (q.lo[k] + q.hi[k]));
+            lo[k] = min(lo[k], key);
+            hi[k] = max(hi[k], key);
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&b[k], lo[k]);
+            atomicMax(&b[3 + k], hi[k]);
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long spread21(unsigned long long v) {
+    v &= 0x1fffffull;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void k_morton(const Box* box, const uint32_t* ids, uint32_t m, const unsigned long long* b,
+                         unsigned long long* code, uint32_t* vals) {
+    double lo[3], ext[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = from_order_key(b[k]);
+        ext[k] = from_order_key(b[3 + k]) - lo[k];
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        uint32_t id = ids[i];
+        const Box& q = box[id];
+        unsigned long long c = 0;
+        for (int k = 0; k < 3; ++k) {
+            double t = ext[k] > 0.0 ? (0.5 * (q.lo[k] + q.hi[k]) - lo[k]) / ext[k] : 0.0;
+            double s = t * 2097152.0;
+            unsigned long long u = s <= 0.0 ? 0ull : (s >= 2097151.0 ? 2097151ull : (unsigned long long)s);
+            c |= spread21(u) << (2 - k);
+        }
+        code[i] = c;
+        vals[i] = id;
+    }
+}
+
+__device__ __forceinline__ int lbvh_delta(const unsigned long long* code, int m, int i, int j) {
+    if (j < 0 || j >= m) return -1;
+    unsigned long long a = code[i], b = code[j];
+    if (a == b) return 64 + __clz((unsigned)(i ^ j));
+    return __clzll(a ^ b);
+}
+
+// Karras 2012, "Maximizing parallelism in the construction of BVHs".
+__global__ void k_karras(const unsigned long long* code, int m, int2* child, int* parent) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m - 1; i += gridDim.x * blockDim.x) {
+        int d = (lbvh_delta(code, m, i, i + 1) - lbvh_delta(code, m, i, i - 1)) >= 0 ? 1 : -1;
+        int dmin = lbvh_delta(code, m, i, i - d);
+        int lmax = 2;
+        while (lbvh_delta(code, m, i, i + lmax * d) > dmin) lmax <<= 1;
+        int l = 0;
+        for (int t = lmax >> 1; t >= 1; t >>= 1)
+            if (lbvh_delta(code, m, i, i + (l + t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = lbvh_delta(code, m, i, j);
+        int s = 0;
+        int t = l;
+        do {
+            t = (t + 1) >> 1;
+            if (lbvh_delta(code, m, i, i + (s + t) * d) > dnode) s += t;
+        } while (t > 1);
+        int gamma = i + s * d + min(d, 0);
+        int left, right;
+        if (min(i, j) == gamma) {
+            left = gamma | 0x80000000;
+            parent[m - 1 + gamma] = i;
+        } else {
+            left = gamma;
+            parent[gamma] = i;
+        }
+        if (max(i, j) == gamma + 1) {
+            right = (gamma + 1) | 0x80000000;
+            parent[m - 1 + gamma + 1] = i;
+        } else {
+            right = gamma + 1;
+            parent[gamma + 1] = i;
+        }
+        child[i] = make_int2(left, right);
+        if (i == 0) parent[0] = -1;
+    }
+}
+
+__global__ void k_lbvh_boxes(const Box* prim_box, const uint32_t* leaf_prim, int m, const int2* child,
+                             const int* parent, unsigned* visits, Box* node_box) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
+        int node = parent[m - 1 + i];
+        while (node >= 0) {
+            __threadfence();
+            if (atomicAdd(&visits[node], 1u) == 0u) break;
+            int2 c = child[node];
+            Box a = (c.x & 0x80000000) ? prim_box[leaf_prim[c.x & 0x7fffffff]] : ldcg_box(&node_box[c.x]);
+            Box b = (c.y & 0x80000000) ? prim_box[leaf_prim[c.y & 0x7fffffff]] : ldcg_box(&node_box[c.y]);
+            node_box[node] = box_union(a, b);
+            node = parent[node];
+        }
+    }
+}
+
+int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaStream_t s) {
+    m = count;
+    if (m == 0) return 0;
+    leaf_prim.reserve(m);
+    ids_tmp.reserve(m);
+    morton.reserve(m);
+    morton_tmp.reserve(m);
+    bounds.reserve(6);
+    node_box.reserve(m > 1 ? m - 1 : 1);
+    child.reserve(m > 1 ? m - 1 : 1);
+    parent.reserve(2 * m);
+    visits.reserve(m);
+    k_bounds_init<<<1, 32, 0, s>>>(bounds.ptr);
+    k_centroid_bounds<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr);
+    k_morton<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr, morton_tmp.ptr, ids_tmp.ptr);
+    size_t need = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, need, morton_tmp.ptr, morton.ptr, ids_tmp.ptr, leaf_prim.ptr, (int)m,
+                                    0, 63, s);
+    if (need > sort_tmp_bytes) {
+        sort_tmp.reserve(need);
+        sort_tmp_bytes = need;
+    }
+    CC_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp.ptr, need, morton_tmp.ptr, morton.ptr, ids_tmp.ptr,
+                                            leaf_prim.ptr, (int)m, 0, 63, s));
+    if (m > 1) {
+        k_karras<<<grid_for(m - 1, 256), 256, 0, s>>>(morton.ptr, (int)m, child.ptr, parent.ptr);
+        CC_CUDA(cudaMemsetAsync(visits.ptr, 0, (m - 1) * sizeof(unsigned), s));
+        k_lbvh_boxes<<<grid_for(m, 256), 256, 0, s>>>(prim_box, leaf_prim.ptr, (int)m, child.ptr, parent.ptr,
+                                                      visits.ptr, node_box.ptr);
+    }
+    CC_CUDA(cudaGetLastError());
+    return m > 1 ? 5 : 3;
+}
+
+// Stack traversal. node_ok(box) prunes internal nodes; leaf_ok(box) is the
+// exact primitive predicate; visit(prim) receives the accepted primitive id.
+template <class NodeOk, class LeafOk, class Visit>
+__device__ __forceinline__ bool lbvh_traverse(const LbvhView& t, NodeOk node_ok, LeafOk leaf_ok, Visit visit) {
+    if (t.m == 0) return true;
+    if (t.m == 1) {
+        uint32_t p = t.leaf_prim[0];
+        if (leaf_ok(t.prim_box[p])) visit(p);
+        return true;
+    }
+    int stack[96];
+    int sp = 0;
+    if (!node_ok(t.node_box[0])) return true;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        int node = stack[--sp];
+        int2 c = t.child[node];
+        int cs[2] = {c.x, c.y};
+        for (int k = 0; k < 2; ++k) {
+            int ch = cs[k];
+            if (ch & 0x80000000) {
+                uint32_t p = t.leaf_prim[ch & 0x7fffffff];
+                if (leaf_ok(t.prim_box[p])) visit(p);
+            } else if (node_ok(t.node_box[ch])) {
+                if (sp >= 96) return false;
+                stack[sp++] = ch;
+            }
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------- geometry
+__device__ __forceinline__ bool adjacent(const WorldView& w, uint32_t a, uint32_t b) {  // world.rs:215-217
+    if (a == b) return true;
+    uint32_t lo = w.ex_off[a], hi = w.ex_off[a + 1];
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t v = w.ex[mid];
+        if (v == b) return true;
+        if (v < b) lo = mid + 1;
+        else hi = mid;
+    }
+    return false;
+}
+
+__device__ bool vertex_feasible(const WorldView& w, d3 p, uint32_t v) {  // geometry.rs:13-17
+    d3 xv = ld3(w.x, v);
+    for (uint32_t k = w.nb_off[v]; k < w.nb_off[v + 1]; ++k) {
+        d3 xj = ld3(w.x, w.nb[k]);
+        if (!(dot(p - xv, xv - xj) >= -1e-14)) return false;
+    }
+    return true;
+}
+
+__device__ bool edge_feasible(const WorldView& w, d3 p, uint32_t e) {  // geometry.rs:18-29
+    uint2 ev = w.edges[e];
+    d3 a = ld3(w.x, ev.x), b = ld3(w.x, ev.y);
+    d3 u = b - a;
+    double t = dot(p - a, u) / len2(u);
+    if (!(t > 0.0 && t < 1.0)) return false;
+    int2 op = w.opposites[e];
+    int ops[2] = {op.x, op.y};
+    for (int k = 0; k < 2; ++k) {
+        if (ops[k] < 0) continue;
+        d3 c = ld3(w.x, (uint32_t)ops[k]);
+        d3 q = a + u * (dot(c - a, u) / len2(u));
+        if (!(dot(p - q, q - c) >= -1e-14)) return false;
+    }
+    return true;
+}
+
+// closest_triangle (geometry.rs:31-77). kind: 0 vertex, 1 edge, 2 face.
+__device__ d3 closest_triangle(const WorldView& w, d3 p, uint32_t t, int& kind, uint32_t& fid) {
+    uint3 ids = w.tri[t];
+    d3 a = ld3(w.x, ids.x), b = ld3(w.x, ids.y), c = ld3(w.x, ids.z);
+    d3 ab = b - a, ac = c - a, ap = p - a;
+    double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0.0 && d2 <= 0.0) {
+        kind = 0;
+        fid = ids.x;
+        return a;
+    }
+    d3 bp = p - b;
+    double d3_ = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3_ >= 0.0 && d4 <= d3_) {
+        kind = 0;
+        fid = ids.y;
+        return b;
+    }
+    double vc = d1 * d4 - d3_ * d2;
+    if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0) {
+        kind = 1;
+        fid = w.tri_edges[t].x;
+        return a + ab * (d1 / (d1 - d3_));
+    }
+    d3 cp = p - c;
+    double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0.0 && d5 <= d6) {
+        kind = 0;
+        fid = ids.z;
+        return c;
+    }
+    double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+        kind = 1;
+        fid = w.tri_edges[t].z;
+        return a + ac * (d2 / (d2 - d6));
+    }
+    double va = d3_ * d6 - d5 * d4;
+    if (va <= 0.0 && d4 - d3_ >= 0.0 && d5 - d6 >= 0.0) {
+        kind = 1;
+        fid = w.tri_edges[t].y;
+        return b + (c - b) * ((d4 - d3_) / ((d4 - d3_) + (d5 - d6)));
+    }
+    double denom = 1.0 / (va + vb + vc);
+    kind = 2;
+    fid = t;
+    return a + ab * (vb * denom) + ac * (vc * denom);
+}
+
+__device__ __forceinline__ double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
+
+// closest_segments (geometry.rs:78-107)
+__device__ void closest_segments(d3 a, d3 b, d3 c, d3 d, double& s_out, double& t_out) {
+    d3 u = b - a;
+    d3 v = d - c;
+    d3 w = a - c;
+    double aa = len2(u);
+    double ee = len2(v);
+    if (aa < 1e-24 || ee < 1e-24) {
+        s_out = 0.0;
+        t_out = 0.0;
+        return;
+    }
+    double bb = dot(u, v);
+    double cc = dot(u, w);
+    double ff = dot(v, w);
+    double den = aa * ee - bb * bb;
+    double s = den > 1e-14 * aa * ee ? clamp01((bb * ff - cc * ee) / den) : 0.0;
+    double t = (bb * s + ff) / ee;
+    if (t < 0.0) {
+        s = clamp01(-cc / aa);
+        t = 0.0;
+    } else if (t > 1.0) {
+        s = clamp01((bb - cc) / aa);
+        t = 1.0;
+    }
+    s_out = s;
+    t_out = t;
+}
+
+// segment_triangle (geometry.rs:131-147)
+__device__ bool segment_triangle(d3 a, d3 b, d3 p, d3 q, d3 r) {
+    d3 e = q - p;
+    d3 f = r - p;
+    d3 d = b - a;
+    d3 h = cross(d, f);
+    double det = dot(e, h);
+    if (fabs(det) < 1e-14) return false;
+    d3 s = a - p;
+    double u = dot(s, h) / det;
+    d3 z = cross(s, e);
+    double v = dot(d, z) / det;
+    double k = dot(f, z) / det;
+    return u >= -1e-10 && v >= -1e-10 && u + v <= 1.0 + 1e-10 && (k >= 1e-10 && k < 1.0 - 1e-10);
+}
+
+// ------------------------------------------------------------ refit/checks
+__global__ void k_refit(WorldView w, const double4* fixed_x, int check_fixed, unsigned int* err) {
+    unsigned int e = 0;
+    size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t i0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (size_t i = i0; i < w.n_all; i += stride) {
+        d3 p = ld3(w.x, (uint32_t)i);
+        if (!isfin(p)) e |= DERR_NONFINITE_STATE;
+        if (check_fixed && i >= w.moving) {
+            double4 f = fixed_x[i - w.moving];
+            if (!(p.x == f.x && p.y == f.y && p.z == f.z)) e |= DERR_FIXED_MOVED;
+        }
+    }
+    for (size_t t = i0; t < w.n_tri; t += stride) {
+        uint3 ids = w.tri[t];
+        d3 a = ld3(w.x, ids.x), b = ld3(w.x, ids.y), c = ld3(w.x, ids.z);
+        Box bx;
+        box_of3(a, b, c, bx);
+        w.tri_box[t] = bx;
+        if (ids.x < w.moving || ids.y < w.moving || ids.z < w.moving) {
+            if (len2(cross(b - a, c - a)) < 1e-24) e |= DERR_DEGENERATE_FACE;
+        }
+    }
+    for (size_t k = i0; k < w.n_edge; k += stride) {
+        uint2 ev = w.edges[k];
+        Box bx;
+        box_of2(ld3(w.x, ev.x), ld3(w.x, ev.y), bx);
+        w.edge_box[k] = bx;
+    }
+    if (e) atomicOr(err, e);
+}
+
+// max_i |x_i - c_i|^2 over moving vertices and max |x| component over all.
+__global__ void k_cover_and_scale(WorldView w, const double4* centers, int have_centers,
+                                  unsigned long long* max_move, unsigned long long* max_abs) {
+    double mm = 0.0, ma = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < w.n_all; i += (size_t)gridDim.x * blockDim.x) {
+        d3 p = ld3(w.x, (uint32_t)i);
+        ma = fmax(ma, fmax(fmax(fabs(p.x), fabs(p.y)), fabs(p.z)));
+        if (have_centers && i < w.moving) {
+            d3 c = ld3(centers, (uint32_t)i);
+            mm = fmax(mm, len2(p - c));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mm = fmax(mm, __shfl_xor_sync(0xffffffffu, mm, o));
+        ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(max_move, dbits(mm));
+        atomicMax(max_abs, dbits(ma));
+    }
+}
+
+// ------------------------------------------------------------ pair queries
+// VF candidates (candidates.rs:29-37): every point against triangles, pairs
+// with box distance <= search, not both fixed, triangle not adjacent.
+__global__ void k_vf_query(WorldView w, LbvhView tri_moving, LbvhView tri_fixed, double search2, uint2* out,
+                           unsigned long long cap, unsigned long long* count, unsigned int* err) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.n_all; v += gridDim.x * blockDim.x) {
+        Box q;
+        box_of1(ld3(w.x, v), q);
+        auto node_ok = [&](const Box& b) { return !(box_dist2(q, b) > search2); };
+        auto leaf_ok = [&](const Box& b) { return box_dist2(q, b) <= search2; };
+        auto visit = [&](uint32_t t) {
+            uint3 ids = w.tri[t];
+            if (adjacent(w, v, ids.x) || adjacent(w, v, ids.y) || adjacent(w, v, ids.z)) return;
+            unsigned long long k = atomicAdd(count, 1ull);
+            if (k < cap) out[k] = make_uint2(v, t);
+        };
+        bool ok = lbvh_traverse(tri_moving, node_ok, leaf_ok, visit);
+        if (v < w.moving) ok = lbvh_traverse(tri_fixed, node_ok, leaf_ok, visit) && ok;
+        if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
+    }
+}
+
+// EE candidates (candidates.rs:38-55): moving edges against moving edges
+// (each unordered pair once, canonical e < f) and against fixed edges
+// (moving edge first).
+__global__ void k_ee_query(WorldView w, const uint32_t* edge_moving, uint32_t n_moving_edges, LbvhView edge_moving_t,
+                           LbvhView edge_fixed_t, double search2, uint2* out, unsigned long long cap,
+                           unsigned long long* count, unsigned int* err) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_moving_edges; k += gridDim.x * blockDim.x) {
+        uint32_t e = edge_moving[k];
+        Box q = w.edge_box[e];
+        uint2 ids = w.edges[e];
+        auto node_ok = [&](const Box& b) { return !(box_dist2(q, b) > search2); };
+        auto leaf_ok = [&](const Box& b) { return box_dist2(q, b) <= search2; };
+        auto filtered = [&](uint32_t f) {
+            uint2 js = w.edges[f];
+            return adjacent(w, ids.x, js.x) || adjacent(w, ids.x, js.y) || adjacent(w, ids.y, js.x) ||
+                   adjacent(w, ids.y, js.y);
+        };
+        auto visit_moving = [&](uint32_t f) {
+            if (f <= e || filtered(f)) return;
+            unsigned long long i = atomicAdd(count, 1ull);
+            if (i < cap) out[i] = make_uint2(e, f);
+        };
+        auto visit_fixed = [&](uint32_t f) {
+            if (filtered(f)) return;
+            unsigned long long i = atomicAdd(count, 1ull);
+            if (i < cap) out[i] = make_uint2(e, f);
+        };
+        bool ok = lbvh_traverse(edge_moving_t, node_ok, leaf_ok, visit_moving);
+        ok = lbvh_traverse(edge_fixed_t, node_ok, leaf_ok, visit_fixed) && ok;
+        if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
+    }
+}
+
+// ------------------------------------------------------------ narrow phase
+__device__ __forceinline__ void push_contact(unsigned kind, uint32_t i0, uint32_t i1, uint32_t i2, uint32_t i3,
+                                             double eps, unsigned long long* hi, unsigned long long* lo,
+                                             double* epsv, uint32_t* idx, unsigned long long cap,
+                                             unsigned long long* count) {
+    // canonical vertex order (world.rs:435-452)
+    uint32_t v[4] = {i0, i1, i2, i3};
+    auto sw = [&](int a, int b) {
+        uint32_t t = v[a];
+        v[a] = v[b];
+        v[b] = t;
+    };
+    if (kind == 0 && v[0] > v[1]) sw(0, 1);
+    if (kind == 1 && v[1] > v[2]) sw(1, 2);
+    if (kind == 2) {
+        if (v[1] > v[2]) sw(1, 2);
+        if (v[2] > v[3]) sw(2, 3);
+        if (v[1] > v[2]) sw(1, 2);
+    }
+    if (kind == 3) {
+        if (v[0] > v[1]) sw(0, 1);
+        if (v[2] > v[3]) sw(2, 3);
+        if (v[0] > v[2]) {
+            sw(0, 2);
+            sw(1, 3);
+        }
+    }
+    unsigned long long k = atomicAdd(count, 1ull);
+    if (k < cap) {
+        hi[k] = ((unsigned long long)kind << 62) | ((unsigned long long)v[0] << 31) | (unsigned long long)v[1];
+        lo[k] = ((unsigned long long)v[2] << 32) | (unsigned long long)v[3];
+        epsv[k] = eps;
+        idx[k] = (uint32_t)k;
+    }
+}
+
+struct NarrowOut {
+    unsigned long long* hi;
+    unsigned long long* lo;
+    double* eps;
+    uint32_t* idx;
+    unsigned long long cap;
+    unsigned long long* count;
+    unsigned long long* dist;  // [n_all] double bits
+    unsigned long long* vf_count;
+    unsigned long long* ee_count;
+    unsigned long long* rejections;
+};
+
+__global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
+                         unsigned long long n_ee, double query_radius, const unsigned long long* max_abs_bits,
+                         int prune, NarrowOut o) {
+    double scale = fmax(query_radius, bitsd(*max_abs_bits));
+    double pr = query_radius + 64.0 * 2.220446049250313e-16 * scale;
+    double padded2 = pr * pr;
+    unsigned long long nvf = 0, nee = 0, nrej = 0;
+    unsigned long long total = n_vf + n_ee;
+    for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (unsigned long long)gridDim.x * blockDim.x) {
+        if (k < n_vf) {
+            uint32_t v = vf[k].x, t = vf[k].y;
+            d3 xv = ld3(w.x, v);
+            if (prune) {
+                Box pb;
+                box_of1(xv, pb);
+                if (box_dist2(pb, w.tri_box[t]) > padded2) {
+                    ++nrej;
+                    continue;
+                }
+            }
+            uint3 ids = w.tri[t];
+            int kind;
+            uint32_t fid;
+            d3 p = closest_triangle(w, xv, t, kind, fid);
+            double d = len(xv - p);
+            if (d >= query_radius) continue;
+            ++nvf;
+            unsigned long long db = dbits(d);
+            atomicMin(&o.dist[v], db);
+            atomicMin(&o.dist[ids.x], db);
+            atomicMin(&o.dist[ids.y], db);
+            atomicMin(&o.dist[ids.z], db);
+            if (kind == 0) {
+                if (vertex_feasible(w, xv, fid))
+                    push_contact(0, v, fid, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+            } else if (kind == 1) {
+                if (edge_feasible(w, xv, fid)) {
+                    uint2 ev = w.edges[fid];
+                    push_contact(1, v, ev.x, ev.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+                }
+            } else {
+                push_contact(2, v, ids.x, ids.y, ids.z, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+            }
+        } else {
+            unsigned long long kk = k - n_vf;
+            uint32_t e = ee[kk].x, f = ee[kk].y;
+            if (prune && box_dist2(w.edge_box[e], w.edge_box[f]) > padded2) {
+                ++nrej;
+                continue;
+            }
+            uint2 ids = w.edges[e], js = w.edges[f];
+            d3 a = ld3(w.x, ids.x), b = ld3(w.x, ids.y), c = ld3(w.x, js.x), dd = ld3(w.x, js.y);
+            double s, t;
+            closest_segments(a, b, c, dd, s, t);
+            d3 p = a + (b - a) * s;
+            d3 q = c + (dd - c) * t;
+            double dist = len(p - q);
+            if (dist >= query_radius) continue;
+            ++nee;
+            unsigned long long db = dbits(dist);
+            atomicMin(&o.dist[ids.x], db);
+            atomicMin(&o.dist[ids.y], db);
+            atomicMin(&o.dist[js.x], db);
+            atomicMin(&o.dist[js.y], db);
+            long end_a = s <= 0.0 ? (long)ids.x : (s >= 1.0 ? (long)ids.y : -1);
+            long end_b = t <= 0.0 ? (long)js.x : (t >= 1.0 ? (long)js.y : -1);
+            if ((end_a >= 0 && !vertex_feasible(w, q, (uint32_t)end_a)) ||
+                (end_b >= 0 && !vertex_feasible(w, p, (uint32_t)end_b)))
+                continue;
+            if (end_a >= 0 && end_b >= 0)
+                push_contact(0, (uint32_t)end_a, (uint32_t)end_b, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap,
+                             o.count);
+            else if (end_a >= 0)
+                push_contact(1, (uint32_t)end_a, js.x, js.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+            else if (end_b >= 0)
+                push_contact(1, (uint32_t)end_b, ids.x, ids.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+            else
+                push_contact(3, ids.x, ids.y, js.x, js.y, 1e-3 * w.rest_len2[e] * w.rest_len2[f], o.hi, o.lo, o.eps,
+                             o.idx, o.cap, o.count);
+        }
+    }
+    for (int s = 16; s > 0; s >>= 1) {
+        nvf += __shfl_xor_sync(0xffffffffu, nvf, s);
+        nee += __shfl_xor_sync(0xffffffffu, nee, s);
+        nrej += __shfl_xor_sync(0xffffffffu, nrej, s);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (nvf) atomicAdd(o.vf_count, nvf);
+        if (nee) atomicAdd(o.ee_count, nee);
+        if (nrej) atomicAdd(o.rejections, nrej);
+    }
+}
+
+__global__ void k_fill_u64(unsigned long long* p, size_t n, unsigned long long v) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+
+__global__ void k_gather_u64(const unsigned long long* src, const uint32_t* idx, unsigned long long* dst, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
+__global__ void k_unique_flags(const unsigned long long* hi, const unsigned long long* lo, size_t n, uint32_t* flag) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        flag[i] = (i == 0 || hi[i] != hi[i - 1] || lo[i] != lo[i - 1]) ? 1u : 0u;
+}
+
+__device__ __forceinline__ uint32_t kind_count(uint32_t kind) { return kind == 0 ? 2u : (kind == 1 ? 3u : 4u); }
+
+// Contact::energy > 0 at the detection configuration (potential.rs:39-65):
+// active iff d < r, and for EE the edges are not parallel (|n|^2 >= 1e-30).
+__device__ bool contact_active(const WorldView& w, uint32_t kind, uint4 v, double r) {
+    d3 p0 = ld3(w.x, v.x), p1 = ld3(w.x, v.y), p2 = ld3(w.x, v.z), p3 = ld3(w.x, v.w);
+    double d;
+    if (kind == 0) {
+        d = len(p0 - p1);
+    } else if (kind == 1) {
+        d3 u = p2 - p1;
+        d3 ww = p0 - p1;
+        double q = dot(ww, u) / dot(u, u);
+        d3 dd = ww - u * q;
+        d = sqrt(dot(dd, dd));
+    } else if (kind == 2) {
+        d3 n = cross(p2 - p1, p3 - p1);
+        double h = dot(p0 - p1, n) / sqrt(dot(n, n));
+        d = h < 0.0 ? -h : h;
+    } else {
+        d3 n = cross(p1 - p0, p3 - p2);
+        if (dot(n, n) < 1e-30) return false;
+        double h = dot(p0 - p2, n) / sqrt(dot(n, n));
+        d = h < 0.0 ? -h : h;
+    }
+    if (d >= r) return false;
+    if (d <= 0.0) return true;  // infinite energy
+    return true;
+}
+
+__global__ void k_compact(const unsigned long long* hi, const unsigned long long* lo, const uint32_t* idx_sorted,
+                          const double* raw_eps, const uint32_t* flag, const uint32_t* pos, size_t n,
+                          uint32_t* c_kind, uint4* c_verts, double* c_eps) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!flag[i]) continue;
+        uint32_t j = pos[i];
+        unsigned long long h = hi[i], l = lo[i];
+        c_kind[j] = (uint32_t)(h >> 62);
+        c_verts[j] = make_uint4((uint32_t)((h >> 31) & 0x7fffffffull), (uint32_t)(h & 0x7fffffffull),
+                                (uint32_t)(l >> 32), (uint32_t)(l & 0xffffffffull));
+        c_eps[j] = raw_eps[idx_sorted[i]];
+    }
+}
+
+__global__ void k_contact_finalize(WorldView w, const uint32_t* c_kind, const uint4* c_verts, size_t n, double r,
+                                   uint32_t* inc_count, unsigned long long* active) {
+    unsigned long long a = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint32_t kind = c_kind[i];
+        uint4 v = c_verts[i];
+        if (contact_active(w, kind, v, r)) ++a;
+        uint32_t vs[4] = {v.x, v.y, v.z, v.w};
+        uint32_t cnt = kind_count(kind);
+        for (uint32_t k = 0; k < cnt; ++k)
+            if (vs[k] < w.moving) atomicAdd(&inc_count[vs[k]], 1u);
+    }
+    for (int s = 16; s > 0; s >>= 1) a += __shfl_xor_sync(0xffffffffu, a, s);
+    if ((threadIdx.x & 31) == 0 && a) atomicAdd(active, a);
+}
+
+// (vertex, contact) keys; sorted, they give every row in ascending contact
+// order, as the reference's incidence lists are (world.rs:386-393).
+__global__ void k_incidence_keys(uint32_t moving, const uint32_t* c_kind, const uint4* c_verts, size_t n,
+                                 unsigned long long* keys, unsigned int* count) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint4 v = c_verts[i];
+        uint32_t vs[4] = {v.x, v.y, v.z, v.w};
+        uint32_t cnt = kind_count(c_kind[i]);
+        for (uint32_t k = 0; k < cnt; ++k)
+            if (vs[k] < moving) {
+                unsigned int slot = atomicAdd(count, 1u);
+                keys[slot] = ((unsigned long long)vs[k] << 32) | (unsigned long long)i;
+            }
+    }
+}
+
+__global__ void k_incidence_extract(const unsigned long long* keys, size_t n, uint32_t* inc) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        inc[i] = (uint32_t)(keys[i] & 0xffffffffull);
+}
+
+__global__ void k_radii(WorldView w, const unsigned long long* dist, double relaxation, double query_radius,
+                        double* radii, double4* centers, unsigned long long* min_bits) {
+    unsigned long long m = dbits(query_radius);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.moving; i += gridDim.x * blockDim.x) {
+        unsigned long long b = dist[i];
+        m = min(m, b);
+        radii[i] = relaxation * bitsd(b);
+        centers[i] = w.x[i];
+    }
+    for (int s = 16; s > 0; s >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, s));
+    if ((threadIdx.x & 31) == 0) atomicMin(min_bits, m);
+}
+
+// validate_start face-face segment tests (world.rs:242-292).
+__global__ void k_intersections(WorldView w, LbvhView tri_moving, LbvhView tri_fixed, const uint32_t* ex_pairs_off,
+                                unsigned long long* first_hit, unsigned int* err) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n_tri; i += gridDim.x * blockDim.x) {
+        uint3 t = w.tri[i];
+        bool t_fixed = t.x >= w.moving && t.y >= w.moving && t.z >= w.moving;
+        Box q = w.tri_box[i];
+        for (int k = 0; k < 3; ++k) {
+            q.lo[k] = q.lo[k] - 1e-10;
+            q.hi[k] = q.hi[k] + 1e-10;
+        }
+        uint32_t tv[3] = {t.x, t.y, t.z};
+        auto visit = [&](uint32_t j) {
+            uint3 qq = w.tri[j];
+            bool q_fixed = qq.x >= w.moving && qq.y >= w.moving && qq.z >= w.moving;
+            if (j <= i || (t_fixed && q_fixed)) return;
+            uint32_t qv[3] = {qq.x, qq.y, qq.z};
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    if (tv[a] != qv[b] && adjacent(w, tv[a], qv[b])) return;
+            auto contains = [](const uint32_t* s, uint32_t v) { return s[0] == v || s[1] == v || s[2] == v; };
+            bool hit = false;
+            for (int k = 0; k < 3; ++k) {
+                bool h1 = !contains(qv, tv[k]) && !contains(qv, tv[(k + 1) % 3]) &&
+                          segment_triangle(ld3(w.x, tv[k]), ld3(w.x, tv[(k + 1) % 3]), ld3(w.x, qv[0]),
+                                           ld3(w.x, qv[1]), ld3(w.x, qv[2]));
+                bool h2 = !contains(tv, qv[k]) && !contains(tv, qv[(k + 1) % 3]) &&
+                          segment_triangle(ld3(w.x, qv[k]), ld3(w.x, qv[(k + 1) % 3]), ld3(w.x, tv[0]),
+                                           ld3(w.x, tv[1]), ld3(w.x, tv[2]));
+                hit = hit || h1 || h2;
+            }
+            if (hit) atomicMin(first_hit, ((unsigned long long)i << 32) | j);
+        };
+        auto node_ok = [&](const Box& b) { return box_overlap(b, q); };
+        auto leaf_ok = [&](const Box& b) { return box_overlap(b, q); };
+        bool ok = lbvh_traverse(tri_moving, node_ok, leaf_ok, visit);
+        if (!t_fixed) ok = lbvh_traverse(tri_fixed, node_ok, leaf_ok, visit) && ok;
+        if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
+    }
+}
+
+// ------------------------------------------------------------------- host
+TopologyHost build_topology(size_t n, const std::vector<std::array<uint32_t, 3>>& tris) {  // topology.rs:13-52
+    TopologyHost top;
+    std::map<std::array<uint32_t, 2>, uint32_t> map;
+    std::vector<std::set<uint32_t>> neighbors(n);
+    std::vector<std::vector<uint32_t>> opp;
+    for (const auto& t : tris) {
+        if (t[0] >= n || t[1] >= n || t[2] >= n || t[0] == t[1] || t[1] == t[2] || t[0] == t[2])
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "OGC: invalid triangle indices"};
+        std::array<uint32_t, 3> te{};
+        for (int k = 0; k < 3; ++k) {
+            uint32_t a = t[k], b = t[(k + 1) % 3], c = t[(k + 2) % 3];
+            std::array<uint32_t, 2> key{std::min(a, b), std::max(a, b)};
+            auto it = map.find(key);
+            uint32_t e;
+            if (it == map.end()) {
+                top.edges.push_back(key);
+                opp.emplace_back();
+                e = (uint32_t)(top.edges.size() - 1);
+                map.emplace(key, e);
+            } else {
+                e = it->second;
+            }
+            opp[e].push_back(c);
+            neighbors[a].insert(b);
+            neighbors[b].insert(a);
+            te[k] = e;
+        }
+        top.tri_edges.push_back(te);
+    }
+    for (const auto& o : opp)
+        if (o.size() > 2)
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "OGC requires manifold triangle edges (at most two incident faces)"};
+    top.tri = tris;
+    top.opposites.resize(opp.size());
+    for (size_t e = 0; e < opp.size(); ++e)
+        top.opposites[e] = {opp[e].size() > 0 ? (int32_t)opp[e][0] : -1, opp[e].size() > 1 ? (int32_t)opp[e][1] : -1};
+    top.nb_off.assign(n + 1, 0);
+    for (size_t i = 0; i < n; ++i) top.nb_off[i + 1] = top.nb_off[i] + (uint32_t)neighbors[i].size();
+    top.nb.reserve(top.nb_off[n]);
+    for (size_t i = 0; i < n; ++i) top.nb.insert(top.nb.end(), neighbors[i].begin(), neighbors[i].end());
+    return top;
+}
+
+World::World(const double* x_all, size_t n_all, const std::vector<std::array<uint32_t, 3>>& tris, size_t moving,
+             const std::vector<std::array<uint32_t, 2>>& excluded, cudaStream_t stream)
+    : stream_(stream), n_all_(n_all), moving_(moving) {
+    if (moving > n_all) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid OGC positions"};
+    for (size_t i = 0; i < 3 * n_all; ++i)
+        if (!std::isfinite(x_all[i])) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid OGC positions"};
+    top_ = build_topology(n_all, tris);
+    n_tri_ = top_.tri.size();
+    n_edge_ = top_.edges.size();
+    auto X = [&](uint32_t i) { return mk(x_all[3 * i], x_all[3 * i + 1], x_all[3 * i + 2]); };
+    for (const auto& t : top_.tri) {
+        d3 a = X(t[0]), b = X(t[1]), c = X(t[2]);
+        if (len2(cross(b - a, c - a)) < 1e-24) throw Failure{CC_ERR_INVALID_ARGUMENT, "OGC degenerate initial face"};
+    }
+    // excluded neighbours, sorted (world.rs:183-197)
+    std::set<std::array<uint32_t, 2>> ex;
+    for (auto e : excluded) ex.insert({std::min(e[0], e[1]), std::max(e[0], e[1])});
+    std::vector<std::vector<uint32_t>> exn(n_all);
+    for (const auto& e : ex) {
+        if (e[1] >= n_all) throw Failure{CC_ERR_INVALID_ARGUMENT, "OGC invalid excluded vertex"};
+        exn[e[0]].push_back(e[1]);
+        exn[e[1]].push_back(e[0]);
+    }
+    std::vector<uint32_t> ex_off(n_all + 1, 0), exv;
+    for (size_t i = 0; i < n_all; ++i) {
+        std::sort(exn[i].begin(), exn[i].end());
+        ex_off[i + 1] = ex_off[i] + (uint32_t)exn[i].size();
+        exv.insert(exv.end(), exn[i].begin(), exn[i].end());
+    }
+    std::vector<double> rl2(n_edge_);
+    for (size_t e = 0; e < n_edge_; ++e) rl2[e] = len2(X(top_.edges[e][0]) - X(top_.edges[e][1]));
+    for (size_t t = 0; t < n_tri_; ++t) {
+        const auto& v = top_.tri[t];
+        (v[0] < moving || v[1] < moving || v[2] < moving ? tri_moving_h_ : tri_fixed_h_).push_back((uint32_t)t);
+    }
+    for (size_t e = 0; e < n_edge_; ++e) {
+        const auto& v = top_.edges[e];
+        (v[0] < moving || v[1] < moving ? edge_moving_h_ : edge_fixed_h_).push_back((uint32_t)e);
+    }
+    std::vector<uint3> tri_d(n_tri_), te_d(n_tri_);
+    for (size_t t = 0; t < n_tri_; ++t) {
+        tri_d[t] = make_uint3(top_.tri[t][0], top_.tri[t][1], top_.tri[t][2]);
+        te_d[t] = make_uint3(top_.tri_edges[t][0], top_.tri_edges[t][1], top_.tri_edges[t][2]);
+    }
+    std::vector<uint2> e_d(n_edge_);
+    std::vector<int2> o_d(n_edge_);
+    for (size_t e = 0; e < n_edge_; ++e) {
+        e_d[e] = make_uint2(top_.edges[e][0], top_.edges[e][1]);
+        o_d[e] = make_int2(top_.opposites[e][0], top_.opposites[e][1]);
+    }
+    std::vector<double4> xh(n_all);
+    for (size_t i = 0; i < n_all; ++i) xh[i] = make_double4(x_all[3 * i], x_all[3 * i + 1], x_all[3 * i + 2], 0.0);
+    tri_.upload(tri_d, stream_);
+    tri_edges_.upload(te_d, stream_);
+    edges_.upload(e_d, stream_);
+    opposites_.upload(o_d, stream_);
+    nb_off_.upload(top_.nb_off, stream_);
+    nb_.upload(top_.nb, stream_);
+    ex_off_.upload(ex_off, stream_);
+    ex_.upload(exv, stream_);
+    rest_len2_.upload(rl2, stream_);
+    x_.upload(xh, stream_);
+    fixed_x_.upload(xh.data() + moving, n_all - moving, stream_);
+    tri_box_.reserve(n_tri_);
+    edge_box_.reserve(n_edge_);
+    tri_moving_.upload(tri_moving_h_, stream_);
+    tri_fixed_.upload(tri_fixed_h_, stream_);
+    edge_moving_.upload(edge_moving_h_, stream_);
+    edge_fixed_.upload(edge_fixed_h_, stream_);
+    dist_bits_.reserve(n_all);
+    radii_.reserve(moving);
+    centers_.reserve(moving);
+    cache_centers_.reserve(moving);
+    inc_count_.reserve(moving + 1);
+    inc_off_.reserve(moving + 1);
+    inc_cursor_.reserve(moving + 1);
+    stats_d_.reserve(1);
+    stats_h_.reserve(1);
+    std::memset(stats_h_.ptr, 0, sizeof(DetectStats));
+    // fixed trees are built once: fixed geometry never moves
+    stats_d_.zero(1, stream_);
+    refit(false);
+    tree_tri_fixed_.build(tri_box_.ptr, tri_fixed_.ptr, (uint32_t)tri_fixed_h_.size(), stream_);
+    tree_edge_fixed_.build(edge_box_.ptr, edge_fixed_.ptr, (uint32_t)edge_fixed_h_.size(), stream_);
+    CC_CUDA(cudaStreamSynchronize(stream_));
+}
+
+World::~World() {}
+
+WorldView World::view() const {
+    return {(uint32_t)n_all_,
+            (uint32_t)moving_,
+            (uint32_t)n_tri_,
+            (uint32_t)n_edge_,
+            tri_.ptr,
+            tri_edges_.ptr,
+            edges_.ptr,
+            opposites_.ptr,
+            nb_off_.ptr,
+            nb_.ptr,
+            ex_off_.ptr,
+            ex_.ptr,
+            rest_len2_.ptr,
+            x_.ptr,
+            tri_box_.ptr,
+            edge_box_.ptr};
+}
+
+ContactsView World::contacts() const {
+    return {(uint32_t)stats_h_.ptr->n_contacts, c_kind_.ptr, c_verts_.ptr, c_eps_.ptr, inc_off_.ptr, inc_.ptr,
+            centers_.ptr, radii_.ptr};
+}
+
+void World::refit(bool check_fixed) {
+    size_t work = std::max(n_all_, std::max(n_tri_, n_edge_));
+    k_refit<<<grid_for(work, 256), 256, 0, stream_>>>(view(), fixed_x_.ptr, check_fixed ? 1 : 0, &stats_d_.ptr->error);
+    ++launches_;
+    CC_CUDA(cudaGetLastError());
+}
+
+void World::sync_stats() {
+    CC_CUDA(cudaMemcpyAsync(stats_h_.ptr, stats_d_.ptr, sizeof(DetectStats), cudaMemcpyDeviceToHost, stream_));
+    CC_CUDA(cudaStreamSynchronize(stream_));
+}
+
+static void raise_device_error(unsigned int e) {
+    if (e & DERR_NONFINITE_STATE) throw Failure{CC_ERR_INVALID_STATE, "OGC invalid position array"};
+    if (e & DERR_FIXED_MOVED) throw Failure{CC_ERR_INVALID_STATE, "OGC fixed geometry changed; rebuild the world"};
+    if (e & DERR_DEGENERATE_FACE) throw Failure{CC_ERR_CONTACT, "OGC degenerate face; step rejected"};
+    if (e & DERR_STACK_OVERFLOW) throw Failure{CC_ERR_CUDA, "OGC LBVH traversal stack overflow"};
+}
+
+void World::build_candidates(double R, double skin) {
+    double search = R + 2.0 * skin + 1e-12;  // candidates.rs:23-28
+    double search2 = search * search;
+    launches_ += tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_);
+    launches_ += tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_);
+    LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
+    LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
+    if (vf_cap_ == 0) {
+        vf_cap_ = std::max<size_t>(1024, 16 * n_all_);
+        ee_cap_ = std::max<size_t>(1024, 32 * n_edge_);
+    }
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        vf_.reserve(vf_cap_);
+        ee_.reserve(ee_cap_);
+        CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_vf, 0, sizeof(unsigned long long), stream_));
+        CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_ee, 0, sizeof(unsigned long long), stream_));
+        k_vf_query<<<grid_for(n_all_, 128), 128, 0, stream_>>>(view(), tm, tf, search2, vf_.ptr, vf_cap_,
+                                                                &stats_d_.ptr->n_vf, &stats_d_.ptr->error);
+        k_ee_query<<<grid_for(edge_moving_h_.size(), 128), 128, 0, stream_>>>(
+            view(), edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), em, ef, search2, ee_.ptr, ee_cap_,
+            &stats_d_.ptr->n_ee, &stats_d_.ptr->error);
+        launches_ += 2;
+        CC_CUDA(cudaGetLastError());
+        sync_stats();
+        raise_device_error(stats_h_.ptr->error);
+        bool grow = false;
+        if (stats_h_.ptr->n_vf > vf_cap_) {
+            vf_cap_ = (size_t)(stats_h_.ptr->n_vf * 1.25) + 1024;
+            vf_.release();
+            grow = true;
+        }
+        if (stats_h_.ptr->n_ee > ee_cap_) {
+            ee_cap_ = (size_t)(stats_h_.ptr->n_ee * 1.25) + 1024;
+            ee_.release();
+            grow = true;
+        }
+        if (!grow) return;
+    }
+    throw Failure{CC_ERR_CUDA, "OGC candidate buffers could not be sized"};
+}
+
+__global__ void k_reset_stats(DetectStats* s, double query_radius) {
+    s->n_raw = 0;
+    s->n_contacts = 0;
+    s->active = 0;
+    s->vf_count = 0;
+    s->ee_count = 0;
+    s->rejections = 0;
+    s->min_dist_bits = dbits(query_radius);
+    s->n_incident = 0;
+    s->max_move_bits = 0;
+    s->max_abs_bits = 0;
+    s->error = 0;
+    s->rebuild = 0;
+}
+
+void World::detect(double query_radius, double radius, double relaxation, double stiffness, bool check_fixed,
+                   bool prune) {
+    (void)stiffness;
+    query_radius_ = query_radius;
+    DetectStats* sd = stats_d_.ptr;
+    // reset per-detection counters (keep n_vf/n_ee of the cache)
+    k_reset_stats<<<1, 1, 0, stream_>>>(sd, query_radius);
+    refit(check_fixed);
+    k_cover_and_scale<<<grid_for(n_all_, 256), 256, 0, stream_>>>(view(), cache_centers_.ptr, cache_valid_ ? 1 : 0,
+                                                                   &sd->max_move_bits, &sd->max_abs_bits);
+    launches_ += 2;
+    CC_CUDA(cudaGetLastError());
+    sync_stats();
+    raise_device_error(stats_h_.ptr->error);
+    double max_move;
+    {
+        unsigned long long b = stats_h_.ptr->max_move_bits;
+        std::memcpy(&max_move, &b, 8);
+    }
+    // Candidates::covers (candidates.rs:15-22)
+    bool rebuild = !(cache_valid_ && query_radius <= cache_R_ && max_move <= cache_skin_ * cache_skin_);
+    if (rebuild) {
+        double R = std::fmax(std::ceil(query_radius / radius) * radius, query_radius);  // world.rs:345
+        build_candidates(R, radius);
+        cache_valid_ = true;
+        cache_R_ = R;
+        cache_skin_ = radius;
+        CC_CUDA(cudaMemcpyAsync(cache_centers_.ptr, x_.ptr, moving_ * sizeof(double4), cudaMemcpyDeviceToDevice,
+                                stream_));
+    }
+    unsigned long long n_vf = stats_h_.ptr->n_vf, n_ee = stats_h_.ptr->n_ee;
+    // narrow phase
+    if (raw_cap_ == 0) raw_cap_ = std::max<size_t>(4096, (size_t)(n_vf + n_ee) / 4 + 4096);
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        raw_hi_.reserve(raw_cap_);
+        raw_lo_.reserve(raw_cap_);
+        raw_eps_.reserve(raw_cap_);
+        raw_idx_.reserve(raw_cap_);
+        CC_CUDA(cudaMemsetAsync(&sd->n_raw, 0, sizeof(unsigned long long), stream_));
+        CC_CUDA(cudaMemsetAsync(&sd->vf_count, 0, sizeof(unsigned long long) * 3, stream_));
+        unsigned long long qbits;
+        std::memcpy(&qbits, &query_radius, 8);
+        k_fill_u64<<<grid_for(n_all_, 256), 256, 0, stream_>>>(dist_bits_.ptr, n_all_, qbits);
+        NarrowOut o{raw_hi_.ptr, raw_lo_.ptr,        raw_eps_.ptr,       raw_idx_.ptr,        raw_cap_,
+                    &sd->n_raw,  dist_bits_.ptr,     &sd->vf_count,      &sd->ee_count,       &sd->rejections};
+        unsigned long long total = n_vf + n_ee;
+        k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee, query_radius,
+                                                                    &sd->max_abs_bits, prune ? 1 : 0, o);
+        launches_ += 2;
+        CC_CUDA(cudaGetLastError());
+        sync_stats();
+        if (stats_h_.ptr->n_raw <= raw_cap_) break;
+        raw_cap_ = (size_t)(stats_h_.ptr->n_raw * 1.25) + 4096;
+        raw_hi_.release();
+        raw_lo_.release();
+        raw_eps_.release();
+        raw_idx_.release();
+    }
+    size_t n_raw = stats_h_.ptr->n_raw;
+    if (n_raw > raw_cap_) throw Failure{CC_ERR_CUDA, "OGC contact buffer could not be sized"};
+    // canonical order: stable LSD radix sort on (lo) then (hi)
+    size_t n_unique = 0;
+    if (n_raw > 0) {
+        raw_hi_s_.reserve(n_raw);
+        raw_lo_s_.reserve(n_raw);
+        raw_idx_s_.reserve(n_raw);
+        uniq_flag_.reserve(n_raw);
+        uniq_pos_.reserve(n_raw);
+        size_t need = 0, need2 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, need, raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_idx_s_.ptr,
+                                        (int)n_raw, 0, 64, stream_);
+        cub::DeviceScan::ExclusiveSum(nullptr, need2, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw, stream_);
+        need = std::max(need, need2);
+        if (need > cub_tmp_bytes_) {
+            cub_tmp_.release();
+            cub_tmp_.reserve(need);
+            cub_tmp_bytes_ = need;
+        }
+        CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.ptr, need, raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr,
+                                                raw_idx_s_.ptr, (int)n_raw, 0, 64, stream_));
+        // gather hi in lo order, then stable sort by hi
+        k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_idx_s_.ptr, raw_hi_s_.ptr, n_raw);
+        CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.ptr, need, raw_hi_s_.ptr, raw_hi_.ptr, raw_idx_s_.ptr,
+                                                raw_idx_.ptr, (int)n_raw, 0, 64, stream_));
+        // raw_hi_ = sorted hi, raw_idx_ = original index; gather lo
+        k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_lo_.ptr, raw_idx_.ptr, raw_lo_s_.ptr, n_raw);
+        k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, n_raw, uniq_flag_.ptr);
+        CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw,
+                                              stream_));
+        uint32_t last_flag = 0, last_pos = 0;
+        CC_CUDA(cudaMemcpyAsync(&last_flag, uniq_flag_.ptr + n_raw - 1, 4, cudaMemcpyDeviceToHost, stream_));
+        CC_CUDA(cudaMemcpyAsync(&last_pos, uniq_pos_.ptr + n_raw - 1, 4, cudaMemcpyDeviceToHost, stream_));
+        CC_CUDA(cudaStreamSynchronize(stream_));
+        n_unique = last_pos + last_flag;
+        c_kind_.reserve(n_unique);
+        c_verts_.reserve(n_unique);
+        c_eps_.reserve(n_unique);
+        k_compact<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_eps_.ptr,
+                                                             uniq_flag_.ptr, uniq_pos_.ptr, n_raw, c_kind_.ptr,
+                                                             c_verts_.ptr, c_eps_.ptr);
+        launches_ += 4;
+    }
+    // incidence (moving vertices), active count, radii
+    CC_CUDA(cudaMemsetAsync(inc_count_.ptr, 0, (moving_ + 1) * sizeof(uint32_t), stream_));
+    CC_CUDA(cudaMemsetAsync(inc_cursor_.ptr, 0, (moving_ + 1) * sizeof(uint32_t), stream_));
+    if (n_unique > 0)
+        k_contact_finalize<<<grid_for(n_unique, 256), 256, 0, stream_>>>(view(), c_kind_.ptr, c_verts_.ptr, n_unique,
+                                                                         radius, inc_count_.ptr, &sd->active);
+    if (n_unique > 0) ++launches_;
+    {
+        size_t need = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1), stream_);
+        if (need > cub_tmp_bytes_) {
+            cub_tmp_.release();
+            cub_tmp_.reserve(need);
+            cub_tmp_bytes_ = need;
+        }
+        CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1),
+                                              stream_));
+    }
+    size_t n_inc_bound = 4 * n_unique;
+    inc_.reserve(std::max<size_t>(n_inc_bound, 1));
+    if (n_unique > 0) {
+        inc_keys_.reserve(n_inc_bound);
+        inc_keys_s_.reserve(n_inc_bound);
+        k_incidence_keys<<<grid_for(n_unique, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
+                                                                        n_unique, inc_keys_.ptr, inc_cursor_.ptr);
+        ++launches_;
+        uint32_t n_inc = 0;
+        CC_CUDA(cudaMemcpyAsync(&n_inc, inc_cursor_.ptr, 4, cudaMemcpyDeviceToHost, stream_));
+        CC_CUDA(cudaStreamSynchronize(stream_));
+        if (n_inc > 0) {
+            size_t need = 0;
+            cub::DeviceRadixSort::SortKeys(nullptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0, 64, stream_);
+            if (need > cub_tmp_bytes_) {
+                cub_tmp_.release();
+                cub_tmp_.reserve(need);
+                cub_tmp_bytes_ = need;
+            }
+            CC_CUDA(cub::DeviceRadixSort::SortKeys(cub_tmp_.ptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0,
+                                                   64, stream_));
+            k_incidence_extract<<<grid_for(n_inc, 256), 256, 0, stream_>>>(inc_keys_s_.ptr, n_inc, inc_.ptr);
+            ++launches_;
+        }
+    }
+    if (moving_ > 0)
+        k_radii<<<grid_for(moving_, 256), 256, 0, stream_>>>(view(), dist_bits_.ptr, relaxation, query_radius,
+                                                             radii_.ptr, centers_.ptr, &sd->min_dist_bits);
+    if (moving_ > 0) ++launches_;
+    CC_CUDA(cudaMemcpyAsync(&sd->n_incident, inc_off_.ptr + moving_, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                            stream_));
+    CC_CUDA(cudaGetLastError());
+    sync_stats();
+    stats_h_.ptr->n_contacts = n_unique;
+    stats_h_.ptr->n_incident &= 0xffffffffull;
+    stats_h_.ptr->rebuild = rebuild ? 1 : 0;
+    raise_device_error(stats_h_.ptr->error);
+}
+
+void World::validate_start() {  // world.rs:242-307
+    CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->error, 0, sizeof(unsigned int), stream_));
+    unsigned long long none = ~0ull;
+    CC_CUDA(cudaMemcpyAsync(&stats_d_.ptr->intersect_key, &none, 8, cudaMemcpyHostToDevice, stream_));
+    refit(true);
+    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_);
+    k_intersections<<<grid_for(n_tri_, 128), 128, 0, stream_>>>(view(), tree_tri_moving_.view(tri_box_.ptr),
+                                                                tree_tri_fixed_.view(tri_box_.ptr), nullptr,
+                                                                &stats_d_.ptr->intersect_key, &stats_d_.ptr->error);
+    CC_CUDA(cudaGetLastError());
+    sync_stats();
+    raise_device_error(stats_h_.ptr->error);
+    unsigned long long hit = stats_h_.ptr->intersect_key;
+    if (hit != ~0ull) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "OGC initial intersection between faces %llu and %llu; reset/rearrange before simulating",
+                      hit >> 32, hit & 0xffffffffull);
+        throw Failure{CC_ERR_CONTACT, buf};
+    }
+    bool was_valid = cache_valid_;
+    double R = cache_R_, skin = cache_skin_;
+    (void)was_valid;
+    (void)R;
+    (void)skin;
+    detect(1e-5, 1e-5, 0.45, 100000.0, true);
+    double md;
+    unsigned long long b = stats_h_.ptr->min_dist_bits;
+    std::memcpy(&md, &b, 8);
+    if (md <= 1e-10)
+        throw Failure{CC_ERR_CONTACT, "OGC initial touching/coplanar features: separation must be positive"};
+}
+
+void World::fresh_pairs(double search, std::vector<uint32_t>& vf, std::vector<uint32_t>& ee) {
+    CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->error, 0, sizeof(unsigned int), stream_));
+    refit(true);
+    sync_stats();
+    raise_device_error(stats_h_.ptr->error);
+    // exact search radius: build_candidates adds 2*skin + 1e-12, so pass R
+    // such that the sum equals `search`
+    double search2 = search * search;
+    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_);
+    tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_);
+    LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
+    LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
+    size_t vcap = std::max<size_t>(1024, 16 * n_all_), ecap = std::max<size_t>(1024, 32 * n_edge_);
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        DBuf<uint2> a, b;
+        a.reserve(vcap);
+        b.reserve(ecap);
+        CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_vf, 0, 16, stream_));
+        k_vf_query<<<grid_for(n_all_, 128), 128, 0, stream_>>>(view(), tm, tf, search2, a.ptr, vcap,
+                                                                &stats_d_.ptr->n_vf, &stats_d_.ptr->error);
+        k_ee_query<<<grid_for(edge_moving_h_.size(), 128), 128, 0, stream_>>>(
+            view(), edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), em, ef, search2, b.ptr, ecap,
+            &stats_d_.ptr->n_ee, &stats_d_.ptr->error);
+        CC_CUDA(cudaGetLastError());
+        sync_stats();
+        raise_device_error(stats_h_.ptr->error);
+        size_t nv = stats_h_.ptr->n_vf, ne = stats_h_.ptr->n_ee;
+        if (nv > vcap || ne > ecap) {
+            vcap = std::max(vcap, nv + 1);
+            ecap = std::max(ecap, ne + 1);
+            continue;
+        }
+        std::vector<uint2> hv(nv), he(ne);
+        if (nv) CC_CUDA(cudaMemcpy(hv.data(), a.ptr, nv * sizeof(uint2), cudaMemcpyDeviceToHost));
+        if (ne) CC_CUDA(cudaMemcpy(he.data(), b.ptr, ne * sizeof(uint2), cudaMemcpyDeviceToHost));
+        std::vector<std::array<uint32_t, 2>> sv(nv), se(ne);
+        for (size_t i = 0; i < nv; ++i) sv[i] = {hv[i].x, hv[i].y};
+        for (size_t i = 0; i < ne; ++i) se[i] = {he[i].x, he[i].y};
+        std::sort(sv.begin(), sv.end());
+        std::sort(se.begin(), se.end());
+        vf.clear();
+        ee.clear();
+        for (auto& p : sv) vf.insert(vf.end(), p.begin(), p.end());
+        for (auto& p : se) ee.insert(ee.end(), p.begin(), p.end());
+        cache_valid_ = false;  // the cache buffers were not touched, but the trees were
+        return;
+    }
+    throw Failure{CC_ERR_CUDA, "OGC candidate buffers could not be sized"};
+}
+
+void World::download(std::vector<uint32_t>& kind, std::vector<uint32_t>& verts, std::vector<double>& eps,
+                     std::vector<uint64_t>& inc_off, std::vector<uint32_t>& inc, std::vector<double>& radii) {
+    size_t n = stats_h_.ptr->n_contacts;
+    kind.resize(n);
+    verts.resize(4 * n);
+    eps.resize(n);
+    if (n) {
+        CC_CUDA(cudaMemcpy(kind.data(), c_kind_.ptr, n * 4, cudaMemcpyDeviceToHost));
+        CC_CUDA(cudaMemcpy(verts.data(), c_verts_.ptr, n * 16, cudaMemcpyDeviceToHost));
+        CC_CUDA(cudaMemcpy(eps.data(), c_eps_.ptr, n * 8, cudaMemcpyDeviceToHost));
+    }
+    std::vector<uint32_t> off(moving_ + 1);
+    CC_CUDA(cudaMemcpy(off.data(), inc_off_.ptr, (moving_ + 1) * 4, cudaMemcpyDeviceToHost));
+    inc_off.assign(off.begin(), off.end());
+    inc.resize(off[moving_]);
+    if (!inc.empty()) CC_CUDA(cudaMemcpy(inc.data(), inc_.ptr, inc.size() * 4, cudaMemcpyDeviceToHost));
+    for (size_t v = 0; v < moving_; ++v) std::sort(inc.begin() + off[v], inc.begin() + off[v + 1]);
+    radii.resize(moving_);
+    if (moving_) CC_CUDA(cudaMemcpy(radii.data(), radii_.ptr, moving_ * 8, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace cc

@@ -1,0 +1,1014 @@
+// VbdSolver on the device and the C ABI of include/clothcraft.h.
+//
+// The step (VbdSolver::step, src/vbd.rs:250-422) runs entirely on the GPU:
+// adaptive initial guess, inertial target, OGC detection, colouring, clipped
+// warm start, colour sweeps with refresh detections, final feasibility and
+// trust-region checks, commit and history record. The host only sequences
+// kernels and reads a few scalars between phases.
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+#include <chrono>
+#include <cmath>
+#include <memory>
+#include <mutex>
+#include <set>
+
+#include "color.cuh"
+#include "sweep.cuh"
+#include "world.cuh"
+
+using namespace cc;
+
+namespace {
+std::mutex g_mutex;
+std::string g_error;
+int g_code = 0;
+int g_device = 0;
+
+int set_global(int code, const std::string& m) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    g_error = m;
+    g_code = code;
+    return code;
+}
+void copy_msg(const std::string& m, char* buf, uint64_t len) {
+    if (buf && len) {
+        size_t k = std::min<size_t>(m.size(), len - 1);
+        std::memcpy(buf, m.data(), k);
+        buf[k] = 0;
+    }
+}
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+bool ogc_valid(const cc_ogc_settings& s) {  // src/ogc/world.rs:56-70
+    return std::isfinite(s.radius) && s.radius > 0.0 && std::isfinite(s.stiffness) && s.stiffness > 0.0 &&
+           std::isfinite(s.relaxation) && s.relaxation > 0.0 && s.relaxation < 0.5 &&
+           std::isfinite(s.refresh_fraction) && s.refresh_fraction >= 0.0 && s.refresh_fraction <= 1.0;
+}
+bool vbd_valid(const cc_vbd_settings& s) {  // src/vbd.rs:38-51
+    return ogc_valid(s.contact) && std::isfinite(s.dt) && s.dt >= 1e-6 && s.dt <= 0.025 && s.iterations != 0 &&
+           s.iterations <= 200 && std::isfinite(s.damping) && s.damping >= 0.0 && std::isfinite(s.gravity[0]) &&
+           std::isfinite(s.gravity[1]) && std::isfinite(s.gravity[2]);
+}
+}  // namespace
+
+// --------------------------------------------------------------- kernels
+namespace cc {
+
+struct StepScalars {
+    unsigned int error;
+    unsigned int mismatch;
+    unsigned int clipped;
+    unsigned int pad;
+    unsigned long long motion_bits;
+    unsigned long long seam_gap_bits;
+    double residual;
+    double ext_total;
+};
+
+__global__ void k_step_begin(uint32_t n, const double4* x0, const double4* v0, const double4* px, const double4* pv,
+                             int has_pred, StepScalars* sc) {
+    unsigned int err = 0, mis = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double4 a = x0[i], b = v0[i];
+        if (!(isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(b.x) && isfinite(b.y) && isfinite(b.z)))
+            err = 1;
+        if (has_pred) {
+            double4 c = px[i], d = pv[i];
+            if (!(a.x == c.x && a.y == c.y && a.z == c.z && b.x == d.x && b.y == d.y && b.z == d.z)) mis = 1;
+        }
+    }
+    if (err) atomicOr(&sc->error, DERR_NONFINITE_STATE);
+    if (mis) atomicOr(&sc->mismatch, 1u);
+}
+
+// Prediction::guess (src/vbd/prediction.rs:15-41), target and inertia
+// (src/vbd.rs:283-302).
+__global__ void k_predict(uint32_t n, const double4* x0, const double4* v0, const double4* accel, int history_ok,
+                          const StepScalars* sc_in, double dt, double3 g, double damping, const double* masses,
+                          double4* guess, double4* target, double* inertia, StepScalars* sc) {
+    bool valid = history_ok && sc_in->mismatch == 0;
+    double g2 = g.x * g.x + g.y * g.y + g.z * g.z;
+    double damp = 1.0 + damping * dt;
+    double dt2 = dt * dt;
+    double mx = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d3 x = ld3(x0, i), v = ld3(v0, i);
+        double factor = 1.0;
+        if (valid && g2 > 1e-20) {
+            d3 a = ld3(accel, i);
+            double f = (a.x * g.x + a.y * g.y + a.z * g.z) / g2;
+            factor = f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
+        }
+        d3 gv = mk(g.x, g.y, g.z);
+        st3(guess, i, x + (v * dt + gv * factor * dt2) / damp);
+        d3 t = x + (v * dt + gv * dt * dt) / damp;
+        st3(target, i, t);
+        inertia[i] = masses[i] * damp / dt2;
+        mx = fmax(mx, len(t - x));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&sc->motion_bits, dbits(mx));
+}
+
+__global__ void k_copy_positions(uint32_t n, const double4* src, double4* dst) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+// Conservative warm start (src/vbd.rs:316-324)
+__global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* guess, ContactsView c, double4* x,
+                             StepScalars* sc) {
+    unsigned int cnt = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (pinned[i]) continue;
+        d3 p = ld3(guess, i);
+        d3 ctr = ld3(c.centers, i);
+        d3 d = p - ctr;
+        double l = len(d);
+        double b = c.radii[i];
+        if (l > b) {
+            p = ctr + d * (b / l);
+            ++cnt;
+        }
+        st3(x, i, p);
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&sc->clipped, cnt);
+}
+
+// finite result and trust-region invariant (src/vbd.rs:399-405), residual sum
+__global__ void k_step_finish(uint32_t n, const double4* x, ContactsView c, const double* residual, StepScalars* sc) {
+    unsigned int err = 0;
+    double r = 0.0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d3 p = ld3(x, i);
+        if (!isfin(p)) err |= DERR_NONFINITE_RESULT;
+        else if (len(p - ld3(c.centers, i)) > c.radii[i] + 1e-10) err |= DERR_TRUST_REGION;
+        r += residual[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&sc->residual, r);
+    if (err) atomicOr(&sc->error, err);
+}
+
+// commit + Prediction::record (src/vbd.rs:406-411, prediction.rs:43-54)
+__global__ void k_commit(uint32_t n, const double4* x, double4* x0, double4* v0, double4* px, double4* pv,
+                         double4* accel, double dt, double damping) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d3 p = ld3(x, i), xo = ld3(x0, i), vo = ld3(v0, i);
+        d3 v = (p - xo) / dt;
+        st3(x0, i, p);
+        st3(v0, i, v);
+        st3(px, i, p);
+        st3(pv, i, v);
+        st3(accel, i, (v - vo) / dt + v * damping);
+    }
+}
+
+// extension_percent inputs (src/garment/diagnostics.rs:7-27) and seam gap
+__global__ void k_stretch(uint32_t nt, const int4* tv, const double4* coef, const double* area, const double4* x,
+                          unsigned long long* key, double* w) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        int4 v = tv[t];
+        double4 cf = coef[t];
+        d3 x0 = ld3(x, v.x), ds0 = ld3(x, v.y) - x0, ds1 = ld3(x, v.z) - x0;
+        d3 ww = ds0 * cf.x + ds1 * cf.y;
+        d3 vv = ds0 * cf.z + ds1 * cf.w;
+        double st = fmax(len(ww), len(vv));
+        double e = 100.0 * fmax(st - 1.0, 0.0);
+        key[t] = order_key(e);
+        w[t] = area[t];
+    }
+}
+
+__global__ void k_p95(uint32_t nt, const unsigned long long* key_sorted, const double* cum, double total,
+                      unsigned long long* out_bits) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        bool hit = cum[t] >= 0.95 * total && (t == 0 || !(cum[t - 1] >= 0.95 * total));
+        if (hit) *out_bits = key_sorted[t];
+    }
+}
+
+__global__ void k_seam_gap(uint32_t ns, const uint32_t* off, const uint32_t* sv, const double* sw, const double4* x,
+                           StepScalars* sc) {
+    double m = 0.0;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) {
+        d3 d = mk(0, 0, 0);
+        for (uint32_t k = off[s]; k < off[s + 1]; ++k) d = d + ld3(x, sv[k]) * sw[k];
+        m = fmax(m, len(d));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&sc->seam_gap_bits, dbits(m));
+}
+
+}  // namespace cc
+
+// ---------------------------------------------------------------- handles
+struct cc_world {
+    std::unique_ptr<World> own;
+    World* w = nullptr;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    std::string err;
+    int code = 0;
+    int fail(const Failure& f) {
+        err = f.message;
+        code = f.code;
+        return f.code;
+    }
+    ~cc_world() {
+        own.reset();
+        if (owns_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct cc_solver {
+    cudaStream_t stream = nullptr;
+    uint32_t n = 0, n_all = 0, n_tri = 0, n_stitch = 0;
+    std::unique_ptr<World> world;
+    cc_world world_view;
+    Coloring coloring;
+    // static sweep data
+    DBuf<int4> tri_v;
+    DBuf<double4> tri_coef;
+    DBuf<double> tri_area;
+    DBuf<MatParams> mats;
+    DBuf<uint4> hinge_v;
+    DBuf<double> hinge_k;
+    DBuf<uint32_t> st_off, st_v;
+    DBuf<double> st_w, st_k;
+    DBuf<uint32_t> inc_off, inc, lo_off, lo;
+    DBuf<uint8_t> pinned;
+    DBuf<double> masses;
+    // state and per-step buffers
+    DBuf<double4> x0, v0, guess, target, pred_x, pred_v, accel;
+    DBuf<double> inertia, residual;
+    DBuf<unsigned char> clipped_flag;
+    DBuf<StepScalars> sc;
+    Pinned<StepScalars> sc_h;
+    Pinned<double4> stage;
+    double time = 0.0;
+    bool has_pred = false;
+    double pred_time = 0.0, pred_damping = 0.0;
+    double pred_g[3] = {0, 0, 0};
+    // metrics scratch
+    DBuf<unsigned long long> ext_key, ext_key_s, p95_bits;
+    DBuf<double> ext_w, ext_w_s, ext_cum;
+    DBuf<unsigned char> cub_tmp;
+    size_t cub_bytes = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool profiling = false;
+    std::vector<cudaEvent_t> prof_events;
+    uint64_t own_launches = 0;
+    uint32_t n_free = 0;
+    std::string err;
+    int code = 0;
+    int fail(const Failure& f) {
+        err = f.message;
+        code = f.code;
+        return f.code;
+    }
+    ~cc_solver() {
+        world.reset();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        for (auto e : prof_events) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    SweepView sweep_view(const ContactsView& cv, const cc_vbd_settings& s, const cc_grab* grab) {
+        SweepView v{};
+        v.n = n;
+        v.x = world->x();
+        v.target = target.ptr;
+        v.inertia = inertia.ptr;
+        v.pinned = pinned.ptr;
+        v.inc_off = inc_off.ptr;
+        v.inc = inc.ptr;
+        v.tri_v = tri_v.ptr;
+        v.tri_coef = tri_coef.ptr;
+        v.tri_area = tri_area.ptr;
+        v.mats = mats.ptr;
+        v.hinge_v = hinge_v.ptr;
+        v.hinge_k = hinge_k.ptr;
+        v.st_off = st_off.ptr;
+        v.st_v = st_v.ptr;
+        v.st_w = st_w.ptr;
+        v.st_k = st_k.ptr;
+        v.contacts = cv;
+        v.contact_r = s.contact.radius;
+        v.contact_k = s.contact.stiffness;
+        v.grab.active = grab ? 1 : 0;
+        if (grab)
+            for (int k = 0; k < 3; ++k) {
+                v.grab.v[k] = grab->vertices[k];
+                v.grab.w[k] = grab->weights[k];
+                v.grab.target[k] = grab->target[k];
+            }
+        v.grab.k = grab ? grab->stiffness : 0.0;
+        v.residual = residual.ptr;
+        v.clipped = &sc.ptr->clipped;
+        v.clipped_flag = clipped_flag.ptr;
+        return v;
+    }
+
+    ColorView color_view(const ContactsView& cv, const cc_grab* grab) {
+        ColorView c{};
+        c.n = n;
+        c.lo_off = lo_off.ptr;
+        c.lo = lo.ptr;
+        c.contacts = cv;
+        c.grab_active = grab ? 1 : 0;
+        if (grab)
+            for (int k = 0; k < 3; ++k) c.grab_v[k] = grab->vertices[k];
+        return c;
+    }
+
+    void read_scalars() {
+        CC_CUDA(cudaMemcpyAsync(sc_h.ptr, sc.ptr, sizeof(StepScalars), cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void detect(double rq, const cc_ogc_settings& s, cc_metrics* m, double& det_ms) {
+        double t = now_ms();
+        world->detect(rq, s.radius, s.relaxation, s.stiffness, false);
+        det_ms += now_ms() - t;
+        if (m) {
+            m->detection_updates += 1;
+            m->broad_phase_rebuilds += world->stats().rebuild;
+            m->candidate_pairs += world->stats().n_vf + world->stats().n_ee;
+            m->aabb_rejections += world->stats().rejections;
+        }
+    }
+
+    void step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out);
+};
+
+void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out) {
+    if (!vbd_valid(s)) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid VBD settings"};
+    if (!std::isfinite(time)) throw Failure{CC_ERR_INVALID_STATE, "Invalid VBD state"};
+    if (grab) {
+        double sum = grab->weights[0] + grab->weights[1] + grab->weights[2];
+        bool bad = !std::isfinite(grab->target[0]) || !std::isfinite(grab->target[1]) ||
+                   !std::isfinite(grab->target[2]) || !std::isfinite(grab->stiffness) || grab->stiffness <= 0.0 ||
+                   std::fabs(sum - 1.0) > 1e-8;
+        for (int i = 0; i < 3; ++i)
+            bad = bad || grab->vertices[i] >= n || !std::isfinite(grab->weights[i]) || grab->weights[i] < 0.0;
+        if (bad) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid mouse attachment"};
+    }
+    double t_start = now_ms();
+    cc_metrics m;
+    std::memset(&m, 0, sizeof m);
+    uint64_t launches0 = own_launches + world->launches() + coloring.launches();
+    size_t prof_used = 0;
+    m.dt_s = s.dt;
+    m.iterations = s.iterations;
+    CC_CUDA(cudaEventRecord(ev0, stream));
+    CC_CUDA(cudaMemsetAsync(sc.ptr, 0, sizeof(StepScalars), stream));
+    int gb = grid_for(n, 256);
+    k_step_begin<<<gb, 256, 0, stream>>>(n, x0.ptr, v0.ptr, pred_x.ptr, pred_v.ptr, has_pred ? 1 : 0, sc.ptr);
+    bool history = has_pred && pred_time == time && pred_g[0] == s.gravity[0] && pred_g[1] == s.gravity[1] &&
+                   pred_g[2] == s.gravity[2] && pred_damping == s.damping;
+    double3 g3 = make_double3(s.gravity[0], s.gravity[1], s.gravity[2]);
+    k_predict<<<gb, 256, 0, stream>>>(n, x0.ptr, v0.ptr, accel.ptr, history ? 1 : 0, sc.ptr, s.dt, g3, s.damping,
+                                      masses.ptr, guess.ptr, target.ptr, inertia.ptr, sc.ptr);
+    own_launches += 2;
+    CC_CUDA(cudaGetLastError());
+    read_scalars();
+    if (sc_h.ptr->error & DERR_NONFINITE_STATE) throw Failure{CC_ERR_INVALID_STATE, "Invalid VBD state"};
+    double motion;
+    std::memcpy(&motion, &sc_h.ptr->motion_bits, 8);
+    double r = s.contact.radius;
+    double rq = std::min(std::max(r + motion, 2.0 * r), 4.0 * r);
+    k_copy_positions<<<gb, 256, 0, stream>>>(n, x0.ptr, world->x());
+    ++own_launches;
+    double det_ms = 0.0;
+    detect(rq, s.contact, &m, det_ms);
+    double md;
+    {
+        unsigned long long b = world->stats().min_dist_bits;
+        std::memcpy(&md, &b, 8);
+    }
+    if (md <= 1e-12) throw Failure{CC_ERR_CONTACT, "OGC zero separation; step rejected, reset the arrangement"};
+    ContactsView cv = world->contacts();
+    coloring.compute(color_view(cv, grab), stream);
+    CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
+    k_warm_start<<<gb, 256, 0, stream>>>(n, pinned.ptr, guess.ptr, cv, world->x(), sc.ptr);
+    ++own_launches;
+    CC_CUDA(cudaGetLastError());
+    read_scalars();
+    size_t clipped = sc_h.ptr->clipped;
+    for (uint32_t it = 0; it < s.iterations; ++it) {
+        if (clipped > 0 && (double)clipped >= s.contact.refresh_fraction * (double)n) {
+            detect(rq, s.contact, &m, det_ms);
+            cv = world->contacts();
+            coloring.compute(color_view(cv, grab), stream);
+        }
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
+        SweepView sv = sweep_view(cv, s, grab);
+        const auto& off = coloring.offsets();
+        for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
+            uint32_t cnt = off[c + 1] - off[c];
+            if (cnt == 0) continue;
+            if (profiling) {
+                while (prof_events.size() < prof_used + 2) {
+                    cudaEvent_t e;
+                    CC_CUDA(cudaEventCreate(&e));
+                    prof_events.push_back(e);
+                }
+                CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
+            }
+            launch_sweep(sv, coloring.order() + off[c], cnt, 1, stream);
+            if (profiling) {
+                CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
+                prof_used += 2;
+            }
+            ++own_launches;
+            ++m.sweep_launches;
+        }
+        m.vertex_solves += n_free;
+        CC_CUDA(cudaGetLastError());
+        read_scalars();
+        clipped = sc_h.ptr->clipped;
+        m.truncated_vertices += clipped;
+    }
+    m.colors = coloring.n_colors();
+    CC_CUDA(cudaMemsetAsync(&sc.ptr->residual, 0, sizeof(double), stream));
+    k_step_finish<<<gb, 256, 0, stream>>>(n, world->x(), cv, residual.ptr, sc.ptr);
+    ++own_launches;
+    CC_CUDA(cudaGetLastError());
+    read_scalars();
+    if (sc_h.ptr->error & DERR_NONFINITE_RESULT) throw Failure{CC_ERR_NON_FINITE, "Non-finite VBD result; state unchanged"};
+    if (sc_h.ptr->error & DERR_TRUST_REGION) throw Failure{CC_ERR_CONTACT, "OGC trust-region invariant failed"};
+    m.residual_rms_n = std::sqrt(sc_h.ptr->residual / (double)(3 * (size_t)n));
+    m.has_residual = 1;
+    k_commit<<<gb, 256, 0, stream>>>(n, world->x(), x0.ptr, v0.ptr, pred_x.ptr, pred_v.ptr, accel.ptr, s.dt,
+                                     s.damping);
+    ++own_launches;
+    time += s.dt;
+    has_pred = true;
+    pred_time = time;
+    pred_damping = s.damping;
+    for (int k = 0; k < 3; ++k) pred_g[k] = s.gravity[k];
+    // metrics: seam gap, extension P95/max
+    if (n_stitch) k_seam_gap<<<grid_for(n_stitch, 256), 256, 0, stream>>>(n_stitch, st_off.ptr, st_v.ptr, st_w.ptr,
+                                                                            x0.ptr, sc.ptr);
+    if (n_stitch) ++own_launches;
+    double p95 = 0.0, emax = 0.0;
+    if (n_tri) {
+        k_stretch<<<grid_for(n_tri, 256), 256, 0, stream>>>(n_tri, tri_v.ptr, tri_coef.ptr, tri_area.ptr, x0.ptr,
+                                                            ext_key.ptr, ext_w.ptr);
+        own_launches += 2;  // k_stretch and k_p95
+        size_t need = 0, need2 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, need, ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr, (int)n_tri,
+                                        0, 64, stream);
+        cub::DeviceScan::InclusiveSum(nullptr, need2, ext_w_s.ptr, ext_cum.ptr, (int)n_tri, stream);
+        need = std::max(need, need2);
+        if (need > cub_bytes) {
+            cub_tmp.release();
+            cub_tmp.reserve(need);
+            cub_bytes = need;
+        }
+        CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.ptr, need, ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr,
+                                                (int)n_tri, 0, 64, stream));
+        CC_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp.ptr, need, ext_w_s.ptr, ext_cum.ptr, (int)n_tri, stream));
+        double total = 0.0;
+        unsigned long long kmax = 0, kp = order_key(0.0);
+        CC_CUDA(cudaMemcpyAsync(&total, ext_cum.ptr + n_tri - 1, 8, cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaMemcpyAsync(&kmax, ext_key_s.ptr + n_tri - 1, 8, cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaStreamSynchronize(stream));
+        CC_CUDA(cudaMemcpyAsync(p95_bits.ptr, &kp, 8, cudaMemcpyHostToDevice, stream));
+        k_p95<<<grid_for(n_tri, 256), 256, 0, stream>>>(n_tri, ext_key_s.ptr, ext_cum.ptr, total, p95_bits.ptr);
+        CC_CUDA(cudaMemcpyAsync(&kp, p95_bits.ptr, 8, cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaStreamSynchronize(stream));
+        p95 = from_order_key(kp);
+        emax = from_order_key(kmax);
+    }
+    CC_CUDA(cudaEventRecord(ev1, stream));
+    read_scalars();
+    float gms = 0.f;
+    CC_CUDA(cudaEventElapsedTime(&gms, ev0, ev1));
+    double gap;
+    std::memcpy(&gap, &sc_h.ptr->seam_gap_bits, 8);
+    m.time_s = time;
+    m.contacts = world->stats().active;
+    m.contact_terms = world->stats().n_contacts;
+    m.minimum_distance_m = md;
+    {
+        unsigned long long b = world->stats().min_dist_bits;
+        std::memcpy(&m.minimum_distance_m, &b, 8);
+    }
+    m.max_seam_gap_m = n_stitch ? gap : 0.0;
+    m.extension_p95_percent = p95;
+    m.extension_max_percent = emax;
+    m.detection_ms = det_ms;
+    m.gpu_compute_ms = gms;
+    if (profiling) {
+        double sw = 0.0;
+        for (size_t k = 0; k < prof_used; k += 2) {
+            float t = 0.f;
+            CC_CUDA(cudaEventElapsedTime(&t, prof_events[k], prof_events[k + 1]));
+            sw += t;
+        }
+        m.sweep_ms = sw;
+    }
+    m.kernel_launches = own_launches + world->launches() + coloring.launches() - launches0;
+    m.contact_incidence = world->stats().n_incident;
+    m.step_ms = now_ms() - t_start;
+    m.solve_ms = m.step_ms - det_ms;
+    if (out) *out = m;
+}
+
+// ----------------------------------------------------------- C entry points
+extern "C" {
+
+int32_t cc_abi_version(void) { return CC_ABI_VERSION; }
+
+int32_t cc_global_last_error(char* buffer, uint64_t length) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    copy_msg(g_error, buffer, length);
+    return g_code;
+}
+
+int32_t cc_last_error(const cc_solver* s, char* buffer, uint64_t length) {
+    copy_msg(s->err, buffer, length);
+    return s->code;
+}
+
+int32_t cc_world_last_error(const cc_world* w, char* buffer, uint64_t length) {
+    copy_msg(w->err, buffer, length);
+    return w->code;
+}
+
+int32_t cc_set_device(int32_t device) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+        return set_global(CC_ERR_CUDA, "cc_set_device: no such CUDA device");
+    g_device = device;
+    return CC_OK;
+}
+
+int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const double* x0, const double* v0,
+                         uint64_t n, cc_solver** out) {
+    try {
+        if (!mesh || !x0 || !out) throw Failure{CC_ERR_INVALID_ARGUMENT, "null argument"};
+        if (mesh->n_vertices != n) throw Failure{CC_ERR_INVALID_ARGUMENT, "VBD state dimensions do not match garment"};
+        CC_CUDA(cudaSetDevice(g_device));
+        auto h = std::make_unique<cc_solver>();
+        CC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        CC_CUDA(cudaEventCreate(&h->ev0));
+        CC_CUDA(cudaEventCreate(&h->ev1));
+        cudaStream_t st = h->stream;
+        h->n = (uint32_t)n;
+        // pins must match their constraints (src/vbd.rs:110-120)
+        for (uint64_t i = 0; i < n; ++i) {
+            if (mesh->pinned && mesh->pinned[i]) {
+                double dx = x0[3 * i] - mesh->pin_positions[3 * i], dy = x0[3 * i + 1] - mesh->pin_positions[3 * i + 1],
+                       dz = x0[3 * i + 2] - mesh->pin_positions[3 * i + 2];
+                if (std::sqrt(dx * dx + dy * dy + dz * dz) > 1e-10)
+                    throw Failure{CC_ERR_INVALID_ARGUMENT,
+                                  "VBD pinned positions must match their constraints before initialization"};
+            }
+        }
+        for (uint64_t i = 0; i < 3 * n; ++i)
+            if (!std::isfinite(x0[i]) || (v0 && !std::isfinite(v0[i])))
+                throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid OGC positions"};
+        // combined positions and faces (src/vbd.rs:121-127)
+        std::vector<double> xall(x0, x0 + 3 * n);
+        std::vector<std::array<uint32_t, 3>> faces;
+        for (uint64_t t = 0; t < mesh->n_triangles; ++t) {
+            std::array<uint32_t, 3> f{mesh->triangles[3 * t], mesh->triangles[3 * t + 1], mesh->triangles[3 * t + 2]};
+            for (uint32_t v : f)
+                if (v >= n) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
+            faces.push_back(f);
+        }
+        if (obstacle) {  // SurfaceMesh::validate (src/avatar.rs:83-98)
+            if (obstacle->n_vertices == 0 || obstacle->n_triangles == 0)
+                throw Failure{CC_ERR_INVALID_ARGUMENT, "Empty/non-finite avatar"};
+            for (uint64_t i = 0; i < 3 * obstacle->n_vertices; ++i)
+                if (!std::isfinite(obstacle->vertices[i])) throw Failure{CC_ERR_INVALID_ARGUMENT, "Empty/non-finite avatar"};
+            for (uint64_t t = 0; t < obstacle->n_triangles; ++t) {
+                uint32_t a = obstacle->triangles[3 * t], b = obstacle->triangles[3 * t + 1],
+                         c = obstacle->triangles[3 * t + 2];
+                if (a >= obstacle->n_vertices || b >= obstacle->n_vertices || c >= obstacle->n_vertices)
+                    throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid avatar index"};
+                auto P = [&](uint32_t i) {
+                    return mk(obstacle->vertices[3 * i], obstacle->vertices[3 * i + 1], obstacle->vertices[3 * i + 2]);
+                };
+                if (len2(cross(P(b) - P(a), P(c) - P(a))) < 1e-24)
+                    throw Failure{CC_ERR_INVALID_ARGUMENT, "Degenerate avatar triangle"};
+                faces.push_back({a + (uint32_t)n, b + (uint32_t)n, c + (uint32_t)n});
+            }
+            xall.insert(xall.end(), obstacle->vertices, obstacle->vertices + 3 * obstacle->n_vertices);
+        }
+        size_t n_all = xall.size() / 3;
+        h->n_all = (uint32_t)n_all;
+        // stitches and their contact exclusions (src/vbd.rs:128-144)
+        std::vector<std::array<uint32_t, 2>> excluded;
+        uint64_t S = mesh->n_stitches;
+        for (uint64_t s = 0; s < S; ++s) {
+            for (uint32_t a = mesh->stitch_offsets[s]; a < mesh->stitch_offsets[s + 1]; ++a) {
+                if (mesh->stitch_vertices[a] >= n) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid seam vertex"};
+                for (uint32_t b = mesh->stitch_offsets[s]; b < mesh->stitch_offsets[s + 1]; ++b)
+                    if (mesh->stitch_weights[a] * mesh->stitch_weights[b] < 0.0)
+                        excluded.push_back({std::min(mesh->stitch_vertices[a], mesh->stitch_vertices[b]),
+                                            std::max(mesh->stitch_vertices[a], mesh->stitch_vertices[b])});
+            }
+        }
+        h->world = std::make_unique<World>(xall.data(), n_all, faces, n, excluded, st);
+        h->world->validate_start();
+        h->world_view.w = h->world.get();
+        h->world_view.stream = st;
+        // materials
+        std::vector<MatParams> mats;
+        for (uint64_t k = 0; k < mesh->n_materials; ++k) {
+            const cc_material& M = mesh->materials[k];
+            mats.push_back({M.warp, M.weft, M.shear, M.compression_ratio, M.compression_transition});
+        }
+        if (mats.empty()) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
+        auto grain = [&](uint32_t mat, double& sn, double& cs) {
+            double r = mesh->materials[mat].grain_degrees * (M_PI / 180.0);
+            sn = std::sin(r);
+            cs = std::cos(r);
+        };
+        // triangles: grain-rotated inverse rest matrix columns
+        uint64_t T = mesh->n_triangles;
+        h->n_tri = (uint32_t)T;
+        std::vector<int4> tv(T);
+        std::vector<double4> tc(T);
+        std::vector<double> ta(T);
+        std::vector<std::vector<uint32_t>> inc(n);
+        std::vector<std::set<uint32_t>> graph(n);
+        auto connect = [&](const uint32_t* ids, size_t k) {
+            for (size_t a = 0; a < k; ++a)
+                for (size_t b = 0; b < k; ++b)
+                    if (ids[a] != ids[b]) graph[ids[a]].insert(ids[b]);
+        };
+        for (uint64_t t = 0; t < T; ++t) {
+            uint32_t mat = mesh->triangle_material ? mesh->triangle_material[t] : 0;
+            if (mat >= mats.size()) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
+            const double* I = mesh->inv_dm + 4 * t;
+            double sn, cs;
+            grain(mat, sn, cs);
+            tv[t] = make_int4((int)mesh->triangles[3 * t], (int)mesh->triangles[3 * t + 1],
+                              (int)mesh->triangles[3 * t + 2], (int)mat);
+            tc[t] = make_double4(I[0] * cs + I[2] * sn, I[1] * cs + I[3] * sn, -I[0] * sn + I[2] * cs,
+                                 -I[1] * sn + I[3] * cs);
+            ta[t] = mesh->area[t];
+            for (uint32_t k = 0; k < 3; ++k) inc[mesh->triangles[3 * t + k]].push_back(pack_term(TERM_TRI, k, (uint32_t)t));
+            connect(mesh->triangles + 3 * t, 3);
+        }
+        uint64_t Hn = mesh->n_hinges;
+        std::vector<uint4> hv(Hn);
+        std::vector<double> hk(Hn);
+        for (uint64_t i = 0; i < Hn; ++i) {
+            const uint32_t* v = mesh->hinges + 4 * i;
+            for (int k = 0; k < 4; ++k)
+                if (v[k] >= n) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
+            uint32_t mat = mesh->hinge_material ? mesh->hinge_material[i] : 0;
+            if (mat >= mats.size()) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
+            double sn, cs;
+            grain(mat, sn, cs);
+            double ax = mesh->hinge_across[2 * i], ay = mesh->hinge_across[2 * i + 1];
+            double aw = ax * cs + ay * sn, af = -ax * sn + ay * cs;
+            const cc_material& M = mesh->materials[mat];
+            hv[i] = make_uint4(v[0], v[1], v[2], v[3]);
+            hk[i] = 0.5 * mesh->hinge_weight[i] * (M.bend_warp * aw * aw + M.bend_weft * af * af);
+            for (uint32_t k = 0; k < 4; ++k) inc[v[k]].push_back(pack_term(TERM_HINGE, k, (uint32_t)i));
+            connect(v, 4);
+        }
+        h->n_stitch = (uint32_t)S;
+        std::vector<uint32_t> so(S + 1, 0), sv;
+        std::vector<double> sw, sk(S);
+        for (uint64_t s = 0; s < S; ++s) {
+            std::vector<uint32_t> ids;
+            for (uint32_t k = mesh->stitch_offsets[s]; k < mesh->stitch_offsets[s + 1]; ++k) {
+                sv.push_back(mesh->stitch_vertices[k]);
+                sw.push_back(mesh->stitch_weights[k]);
+                ids.push_back(mesh->stitch_vertices[k]);
+            }
+            so[s + 1] = (uint32_t)sv.size();
+            sk[s] = mesh->stitch_stiffness[s];
+            for (uint32_t v : ids) inc[v].push_back(pack_term(TERM_STITCH, 0, (uint32_t)s));
+            connect(ids.data(), ids.size());
+        }
+        std::vector<uint32_t> io(n + 1, 0), iv, lo_o(n + 1, 0), lo_v;
+        for (uint64_t v = 0; v < n; ++v) {
+            io[v + 1] = io[v] + (uint32_t)inc[v].size();
+            iv.insert(iv.end(), inc[v].begin(), inc[v].end());
+            for (uint32_t u : graph[v])
+                if (u < v) lo_v.push_back(u);
+            lo_o[v + 1] = (uint32_t)lo_v.size();
+        }
+        std::vector<uint8_t> pin(n, 0);
+        if (mesh->pinned)
+            for (uint64_t i = 0; i < n; ++i) pin[i] = mesh->pinned[i] ? 1 : 0;
+        h->n_free = 0;
+        for (uint64_t i = 0; i < n; ++i) h->n_free += pin[i] ? 0 : 1;
+        for (uint64_t i = 0; i < n; ++i)
+            if (!(mesh->masses[i] > 0.0) || !std::isfinite(mesh->masses[i]))
+                throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
+        h->mats.upload(mats, st);
+        h->tri_v.upload(tv, st);
+        h->tri_coef.upload(tc, st);
+        h->tri_area.upload(ta, st);
+        h->hinge_v.upload(hv, st);
+        h->hinge_k.upload(hk, st);
+        h->st_off.upload(so, st);
+        h->st_v.upload(sv, st);
+        h->st_w.upload(sw, st);
+        h->st_k.upload(sk, st);
+        h->inc_off.upload(io, st);
+        h->inc.upload(iv, st);
+        h->lo_off.upload(lo_o, st);
+        h->lo.upload(lo_v, st);
+        h->pinned.upload(pin, st);
+        h->masses.upload(mesh->masses, n, st);
+        for (auto* b : {&h->x0, &h->v0, &h->guess, &h->target, &h->pred_x, &h->pred_v, &h->accel}) b->reserve(n);
+        h->inertia.reserve(n);
+        h->residual.reserve(n);
+        h->clipped_flag.reserve(n);
+        h->sc.reserve(1);
+        h->sc_h.reserve(1);
+        h->stage.reserve(2 * n);
+        h->ext_key.reserve(T);
+        h->ext_key_s.reserve(T);
+        h->ext_w.reserve(T);
+        h->ext_w_s.reserve(T);
+        h->ext_cum.reserve(T);
+        h->p95_bits.reserve(1);
+        h->residual.zero(n, st);
+        h->coloring.init((uint32_t)n, st);
+        // initial state
+        for (uint64_t i = 0; i < n; ++i) {
+            h->stage.ptr[i] = make_double4(x0[3 * i], x0[3 * i + 1], x0[3 * i + 2], 0.0);
+            h->stage.ptr[n + i] = v0 ? make_double4(v0[3 * i], v0[3 * i + 1], v0[3 * i + 2], 0.0) : make_double4(0, 0, 0, 0);
+        }
+        CC_CUDA(cudaMemcpyAsync(h->x0.ptr, h->stage.ptr, n * sizeof(double4), cudaMemcpyHostToDevice, st));
+        CC_CUDA(cudaMemcpyAsync(h->v0.ptr, h->stage.ptr + n, n * sizeof(double4), cudaMemcpyHostToDevice, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        *out = h.release();
+        return CC_OK;
+    } catch (const Failure& f) {
+        return set_global(f.code, f.message);
+    } catch (const std::exception& e) {
+        return set_global(CC_ERR_CUDA, e.what());
+    }
+}
+
+void cc_solver_destroy(cc_solver* s) { delete s; }
+uint64_t cc_solver_moving(const cc_solver* s) { return s->n; }
+uint64_t cc_solver_total(const cc_solver* s) { return s->n_all; }
+void* cc_solver_stream(const cc_solver* s) { return (void*)s->stream; }
+int32_t cc_solver_set_profiling(cc_solver* s, int32_t enable) {
+    s->profiling = enable != 0;
+    return CC_OK;
+}
+cc_world* cc_solver_world(cc_solver* s) { return &s->world_view; }
+
+static void upload_state(cc_solver* s, const double* x, const double* v) {
+    size_t n = s->n;
+    for (size_t i = 0; i < n; ++i) {
+        s->stage.ptr[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0);
+        s->stage.ptr[n + i] = make_double4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0);
+    }
+    CC_CUDA(cudaMemcpyAsync(s->x0.ptr, s->stage.ptr, n * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
+    CC_CUDA(cudaMemcpyAsync(s->v0.ptr, s->stage.ptr + n, n * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
+}
+
+static void download_state(cc_solver* s, double* x, double* v) {
+    size_t n = s->n;
+    CC_CUDA(cudaMemcpyAsync(s->stage.ptr, s->x0.ptr, n * sizeof(double4), cudaMemcpyDeviceToHost, s->stream));
+    CC_CUDA(cudaMemcpyAsync(s->stage.ptr + n, s->v0.ptr, n * sizeof(double4), cudaMemcpyDeviceToHost, s->stream));
+    CC_CUDA(cudaStreamSynchronize(s->stream));
+    for (size_t i = 0; i < n; ++i) {
+        double4 a = s->stage.ptr[i], b = s->stage.ptr[n + i];
+        x[3 * i] = a.x;
+        x[3 * i + 1] = a.y;
+        x[3 * i + 2] = a.z;
+        v[3 * i] = b.x;
+        v[3 * i + 1] = b.y;
+        v[3 * i + 2] = b.z;
+    }
+}
+
+int32_t cc_solver_set_state(cc_solver* s, const double* x, const double* v, double time) {
+    try {
+        upload_state(s, x, v);
+        s->time = time;
+        CC_CUDA(cudaStreamSynchronize(s->stream));
+        return CC_OK;
+    } catch (const Failure& f) {
+        return s->fail(f);
+    }
+}
+
+int32_t cc_solver_get_state(cc_solver* s, double* x, double* v, double* time) {
+    try {
+        download_state(s, x, v);
+        if (time) *time = s->time;
+        return CC_OK;
+    } catch (const Failure& f) {
+        return s->fail(f);
+    }
+}
+
+int32_t cc_solver_step_resident(cc_solver* s, const cc_vbd_settings* settings, const cc_grab* grab,
+                                cc_metrics* metrics) {
+    // The resident state is the last committed one; a failed step leaves it
+    // (and the prediction history) untouched.
+    double t0 = s->time;
+    try {
+        s->step(*settings, grab, metrics);
+        return CC_OK;
+    } catch (const Failure& f) {
+        s->time = t0;
+        return s->fail(f);
+    }
+}
+
+int32_t cc_solver_step(cc_solver* s, double* x, double* v, double* time, const cc_vbd_settings* settings,
+                       const cc_grab* grab, cc_metrics* metrics) {
+    try {
+        upload_state(s, x, v);
+        s->time = *time;
+        s->step(*settings, grab, metrics);
+        download_state(s, x, v);
+        *time = s->time;
+        return CC_OK;
+    } catch (const Failure& f) {
+        return s->fail(f);
+    }
+}
+
+static void upload_all(World* w, const double* x_all, cudaStream_t st, Pinned<double4>& stage) {
+    size_t N = w->n_all();
+    stage.reserve(N);
+    for (size_t i = 0; i < N; ++i) stage.ptr[i] = make_double4(x_all[3 * i], x_all[3 * i + 1], x_all[3 * i + 2], 0.0);
+    CC_CUDA(cudaMemcpyAsync(w->x(), stage.ptr, N * sizeof(double4), cudaMemcpyHostToDevice, st));
+    CC_CUDA(cudaStreamSynchronize(st));
+}
+
+int32_t cc_solver_colors(cc_solver* s, const double* x_all, double query_radius, const cc_ogc_settings* settings,
+                         const cc_grab* grab, uint32_t* colors_out, uint32_t* n_colors) {
+    try {
+        if (!ogc_valid(*settings)) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid OGC radius, stiffness or trust-region parameters"};
+        Pinned<double4> stage;
+        upload_all(s->world.get(), x_all, s->stream, stage);
+        s->world->detect(query_radius, settings->radius, settings->relaxation, settings->stiffness, true);
+        s->coloring.compute(s->color_view(s->world->contacts(), grab), s->stream);
+        std::vector<uint32_t> c;
+        s->coloring.download(c);
+        std::copy(c.begin(), c.end(), colors_out);
+        *n_colors = s->coloring.n_colors();
+        return CC_OK;
+    } catch (const Failure& f) {
+        return s->fail(f);
+    }
+}
+
+int32_t cc_solver_local_blocks(cc_solver* s, const double* x_all, double query_radius,
+                               const cc_vbd_settings* settings, const cc_grab* grab, const double* targets,
+                               const double* inertia, double* energy, double* gradient, double* hessian) {
+    try {
+        if (!ogc_valid(settings->contact))
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid OGC radius, stiffness or trust-region parameters"};
+        Pinned<double4> stage;
+        upload_all(s->world.get(), x_all, s->stream, stage);
+        size_t n = s->n;
+        if (targets) {
+            std::vector<double4> t(n);
+            for (size_t i = 0; i < n; ++i) t[i] = make_double4(targets[3 * i], targets[3 * i + 1], targets[3 * i + 2], 0);
+            s->target.upload(t, s->stream);
+        }
+        if (inertia) s->inertia.upload(inertia, n, s->stream);
+        s->world->detect(query_radius, settings->contact.radius, settings->contact.relaxation,
+                         settings->contact.stiffness, true);
+        SweepView sv = s->sweep_view(s->world->contacts(), *settings, grab);
+        if (!targets) sv.target = nullptr;
+        if (!inertia) sv.inertia = nullptr;
+        DBuf<double> e, g, h;
+        e.reserve(n);
+        g.reserve(3 * n);
+        h.reserve(9 * n);
+        launch_local_blocks(sv, e.ptr, g.ptr, h.ptr, s->stream);
+        CC_CUDA(cudaGetLastError());
+        CC_CUDA(cudaMemcpyAsync(energy, e.ptr, n * 8, cudaMemcpyDeviceToHost, s->stream));
+        CC_CUDA(cudaMemcpyAsync(gradient, g.ptr, 3 * n * 8, cudaMemcpyDeviceToHost, s->stream));
+        CC_CUDA(cudaMemcpyAsync(hessian, h.ptr, 9 * n * 8, cudaMemcpyDeviceToHost, s->stream));
+        CC_CUDA(cudaStreamSynchronize(s->stream));
+        return CC_OK;
+    } catch (const Failure& f) {
+        return s->fail(f);
+    }
+}
+
+int32_t cc_world_create(const double* x, uint64_t n_all, const uint32_t* triangles, uint64_t n_triangles,
+                        uint64_t moving, const uint32_t* excluded, uint64_t n_excluded, cc_world** out) {
+    try {
+        CC_CUDA(cudaSetDevice(g_device));
+        auto h = std::make_unique<cc_world>();
+        CC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->owns_stream = true;
+        std::vector<std::array<uint32_t, 3>> tris(n_triangles);
+        for (uint64_t t = 0; t < n_triangles; ++t) tris[t] = {triangles[3 * t], triangles[3 * t + 1], triangles[3 * t + 2]};
+        std::vector<std::array<uint32_t, 2>> ex(n_excluded);
+        for (uint64_t e = 0; e < n_excluded; ++e) ex[e] = {excluded[2 * e], excluded[2 * e + 1]};
+        h->own = std::make_unique<World>(x, n_all, tris, moving, ex, h->stream);
+        h->w = h->own.get();
+        *out = h.release();
+        return CC_OK;
+    } catch (const Failure& f) {
+        return set_global(f.code, f.message);
+    }
+}
+
+void cc_world_destroy(cc_world* w) {
+    if (w && w->own) delete w;
+}
+
+int32_t cc_world_validate_start(cc_world* w, const double* x) {
+    try {
+        Pinned<double4> stage;
+        upload_all(w->w, x, w->w->stream(), stage);
+        w->w->validate_start();
+        return CC_OK;
+    } catch (const Failure& f) {
+        return w->fail(f);
+    }
+}
+
+int32_t cc_world_detect(cc_world* w, const double* x, double query_radius, const cc_ogc_settings* settings,
+                        cc_contacts* out) {
+    try {
+        if (!ogc_valid(*settings))
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid OGC radius, stiffness or trust-region parameters"};
+        if (!std::isfinite(query_radius) || query_radius < settings->radius)
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "OGC query radius must cover the contact radius"};
+        Pinned<double4> stage;
+        upload_all(w->w, x, w->w->stream(), stage);
+        w->w->detect(query_radius, settings->radius, settings->relaxation, settings->stiffness, true);
+        const DetectStats& st = w->w->stats();
+        std::vector<uint32_t> kind, verts, inc;
+        std::vector<double> eps, radii;
+        std::vector<uint64_t> inc_off;
+        w->w->download(kind, verts, eps, inc_off, inc, radii);
+        size_t moving = w->w->moving();
+        out->n_contacts = kind.size();
+        out->n_incident = inc.size();
+        out->active_contacts = st.active;
+        out->vertex_face_candidates = st.vf_count;
+        out->edge_edge_candidates = st.ee_count;
+        out->candidate_pairs = st.n_vf + st.n_ee;
+        out->aabb_rejections = st.rejections;
+        std::memcpy(&out->minimum_distance, &st.min_dist_bits, 8);
+        out->broad_phase_rebuilt = st.rebuild ? 1 : 0;
+        if (out->contact_capacity < kind.size() || out->incident_capacity < inc.size() || out->radii_capacity < moving)
+            return CC_ERR_CAPACITY;
+        for (size_t c = 0; c < kind.size(); ++c) {
+            if (out->kinds) out->kinds[c] = (uint8_t)kind[c];
+            if (out->vertices)
+                for (int k = 0; k < 4; ++k) out->vertices[4 * c + k] = verts[4 * c + k];
+            if (out->counts) out->counts[c] = (uint8_t)(kind[c] == 0 ? 2 : (kind[c] == 1 ? 3 : 4));
+            if (out->mollifier_epsilon) out->mollifier_epsilon[c] = eps[c];
+        }
+        if (out->incident_offsets) std::copy(inc_off.begin(), inc_off.end(), out->incident_offsets);
+        if (out->incident) std::copy(inc.begin(), inc.end(), out->incident);
+        if (out->radii) std::copy(radii.begin(), radii.end(), out->radii);
+        return CC_OK;
+    } catch (const Failure& f) {
+        return w->fail(f);
+    }
+}
+
+int32_t cc_world_candidates(cc_world* w, const double* x, double radius, cc_candidates* out) {
+    try {
+        Pinned<double4> stage;
+        upload_all(w->w, x, w->w->stream(), stage);
+        std::vector<uint32_t> vf, ee;
+        w->w->fresh_pairs(radius, vf, ee);
+        out->n_vf = vf.size() / 2;
+        out->n_ee = ee.size() / 2;
+        if (out->vf_capacity < out->n_vf || out->ee_capacity < out->n_ee) return CC_ERR_CAPACITY;
+        std::copy(vf.begin(), vf.end(), out->vf);
+        std::copy(ee.begin(), ee.end(), out->ee);
+        return CC_OK;
+    } catch (const Failure& f) {
+        return w->fail(f);
+    }
+}
+
+uint64_t cc_world_edges(const cc_world* w, uint32_t* edges_out) {
+    const auto& e = w->w->topology().edges;
+    if (edges_out)
+        for (size_t i = 0; i < e.size(); ++i) {
+            edges_out[2 * i] = e[i][0];
+            edges_out[2 * i + 1] = e[i][1];
+        }
+    return e.size();
+}
+
+}  // extern "C"

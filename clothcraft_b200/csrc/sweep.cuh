@@ -1,0 +1,55 @@
+// VBD colour-sweep data layout and kernel entry points.
+#pragma once
+#include "world.cuh"
+
+namespace cc {
+
+struct MatParams {  // per material, membrane part (src/energy.rs:10-29)
+    double warp, weft, shear, c, delta;
+};
+
+// Packed incidence entry: type (2 bits) | slot (2 bits) | index (28 bits).
+enum TermType : uint32_t { TERM_TRI = 0, TERM_HINGE = 1, TERM_STITCH = 2 };
+__host__ __device__ inline uint32_t pack_term(uint32_t type, uint32_t slot, uint32_t idx) {
+    return (type << 30) | (slot << 28) | idx;
+}
+
+struct GrabDev {
+    int active;
+    uint32_t v[3];
+    double w[3];
+    double target[3];
+    double k;
+};
+
+struct SweepView {
+    uint32_t n;                 // moving vertices
+    double4* x;                 // [n_all] positions (moving part written)
+    const double4* target;      // [n]
+    const double* inertia;      // [n]
+    const uint8_t* pinned;      // [n]
+    const uint32_t* inc_off;    // [n+1] static incidence
+    const uint32_t* inc;
+    const int4* tri_v;          // v0, v1, v2, material
+    const double4* tri_coef;    // w = ds0*c.x + ds1*c.y ; v = ds0*c.z + ds1*c.w (grain-rotated inv_dm)
+    const double* tri_area;
+    const MatParams* mats;
+    const uint4* hinge_v;
+    const double* hinge_k;      // 0.5 * weight * (bend_warp aw^2 + bend_weft af^2)
+    const uint32_t* st_off;
+    const uint32_t* st_v;
+    const double* st_w;
+    const double* st_k;
+    ContactsView contacts;
+    double contact_r, contact_k;
+    GrabDev grab;
+    double* residual;           // [n] |g|^2 of the vertex's last solve
+    unsigned int* clipped;      // counter
+    unsigned char* clipped_flag;  // [n]
+};
+
+// launch helpers (sweep.cu)
+void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
+void launch_local_blocks(const SweepView& s, double* energy, double* grad, double* hess, cudaStream_t st);
+
+}  // namespace cc

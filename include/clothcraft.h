@@ -128,6 +128,12 @@ typedef struct cc_metrics {
     double residual_rms_n;
     int32_t has_residual;           /* 1 when residual_rms_n is defined       */
     int32_t reserved0;
+    /* device-side accounting of the step (no reference counterpart) */
+    double sweep_ms;                /* colour-sweep kernel time (profiling on) */
+    uint64_t sweep_launches;        /* colour-sweep kernel launches           */
+    uint64_t vertex_solves;         /* local solves: free vertices x sweeps   */
+    uint64_t kernel_launches;       /* launches of this library's kernels     */
+    uint64_t contact_incidence;     /* entries of the last contact incidence  */
 } cc_metrics;
 
 /* ContactSet (src/ogc/world.rs:73-107) in caller-owned arrays. The contact
@@ -209,6 +215,15 @@ int32_t cc_solver_step_resident(cc_solver* solver, const cc_vbd_settings* settin
 /* Number of cloth (moving) vertices and of all vertices including the obstacle. */
 uint64_t cc_solver_moving(const cc_solver* solver);
 uint64_t cc_solver_total(const cc_solver* solver);
+
+/* The CUDA stream (cudaStream_t) every kernel of this solver is launched on,
+ * for callers that time the step with CUDA events. No reference counterpart
+ * (the wgpu backend times its compute pass with timestamp queries,
+ * src/gpu_vbd/cache.rs:16-33). */
+void* cc_solver_stream(const cc_solver* solver);
+/* When enabled, each colour-sweep launch is bracketed by CUDA events and
+ * cc_metrics.sweep_ms reports their summed device time. */
+int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
 
 /* The solver's OGC world (owned by the solver; do not destroy). */
 cc_world* cc_solver_world(cc_solver* solver);

@@ -19,6 +19,7 @@ from pathlib import Path
 import numpy as np
 
 from clothcraft_b200 import abi
+from clothcraft_b200.abi import read_contacts, ContactResult  # noqa: F401
 from clothcraft_b200.abi import (c_double_p, c_uint32_p, c_uint8_p, c_uint64_p, cc_candidates, cc_contacts,
                                  cc_grab, cc_mesh, cc_metrics, cc_ogc_settings, cc_surface, cc_vbd_settings)
 
@@ -136,49 +137,6 @@ def grab_c(grab):
 
 def _byref_or_null(obj, ctype):
     return C.byref(obj) if obj is not None else C.cast(None, C.POINTER(ctype))
-
-
-class ContactResult(dict):
-    """ContactSet fields as numpy arrays / scalars."""
-
-
-def read_contacts(call, moving: int, contact_hint: int = 4096) -> ContactResult:
-    """Two-call protocol around a cc_contacts-filling function."""
-    cap = contact_hint
-    while True:
-        out = cc_contacts()
-        kinds = np.zeros(cap, np.uint8)
-        verts = np.zeros((cap, 4), np.uint32)
-        counts = np.zeros(cap, np.uint8)
-        eps = np.zeros(cap)
-        inc_off = np.zeros(moving + 1, np.uint64)
-        inc = np.zeros(4 * cap, np.uint32)
-        radii = np.zeros(max(moving, 1))
-        out.contact_capacity = cap
-        out.incident_capacity = 4 * cap
-        out.radii_capacity = moving
-        out.kinds = abi.ptr(kinds, C.c_uint8)
-        out.vertices = abi.ptr(verts, C.c_uint32)
-        out.counts = abi.ptr(counts, C.c_uint8)
-        out.mollifier_epsilon = abi.ptr(eps, C.c_double)
-        out.incident_offsets = abi.ptr(inc_off, C.c_uint64)
-        out.incident = abi.ptr(inc, C.c_uint32)
-        out.radii = abi.ptr(radii, C.c_double)
-        rc = call(out)
-        if rc == abi.CC_ERR_CAPACITY:
-            cap = max(int(out.n_contacts), int(out.n_incident) // 4 + 1, 2 * cap)
-            continue
-        if rc != abi.CC_OK:
-            return rc
-        k = int(out.n_contacts)
-        r = ContactResult(
-            kinds=kinds[:k].copy(), vertices=verts[:k].copy(), counts=counts[:k].copy(), epsilon=eps[:k].copy(),
-            incident_offsets=inc_off.copy(), incident=inc[:int(out.n_incident)].copy(), radii=radii[:moving].copy(),
-            active_contacts=int(out.active_contacts), vertex_face_candidates=int(out.vertex_face_candidates),
-            edge_edge_candidates=int(out.edge_edge_candidates), candidate_pairs=int(out.candidate_pairs),
-            aabb_rejections=int(out.aabb_rejections), minimum_distance=float(out.minimum_distance),
-            broad_phase_rebuilt=bool(out.broad_phase_rebuilt))
-        return r
 
 
 class World:

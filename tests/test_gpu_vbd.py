@@ -1,0 +1,215 @@
+"""GPU VBD step parity against the oracle, through the C ABI.
+
+Bars (from the hot-path contract):
+  (a) per-vertex positions after one step within 1e-5 m of the CPU path;
+  (b) energy and force residual within 1 % after many steps;
+  plus the reference's own VBD known-answer tests run on the GPU backend.
+Local blocks (energy, gradient, Hessian) and colourings are compared at
+identical positions: colours exactly, blocks to 1e-9 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from clothcraft_b200 import scenes
+from clothcraft_b200.vbd import VbdError, VbdSolver
+
+pytestmark = pytest.mark.gpu
+
+POSITION_TOL_M = 1e-5      # (a)
+RELATIVE_TOL = 0.01        # (b)
+BLOCK_RTOL = 1e-9
+
+
+def contact_scene(n=16, seed=0):
+    """Small sheet 4 mm above a sphere so contacts appear within a few steps."""
+    return scenes.small_sheet(n, seed=seed, height=0.104, side=0.2, pins=(), radius=0.002)
+
+
+def run_both(sc, steps, settings=None):
+    st = (settings or sc.settings).to_c()
+    g = VbdSolver(sc)
+    o = oracle.Solver(sc, threads=8)
+    xg, vg, tg = sc.x0.copy(), sc.v0.copy(), 0.0
+    xo, vo, to = sc.x0.copy(), sc.v0.copy(), 0.0
+    out = []
+    for _ in range(steps):
+        xg, vg, tg, mg = g.step(xg, vg, tg, st)
+        xo, vo, to, mo = o.step(xo, vo, to, st)
+        out.append((xg.copy(), xo.copy(), mg, mo))
+    return out, g, o
+
+
+def test_local_blocks_match_oracle_jet_ad():
+    sc = contact_scene()
+    g = VbdSolver(sc)
+    o = oracle.Solver(sc)
+    rng = np.random.default_rng(0)
+    st = sc.settings.to_c()
+    x = sc.x0.copy()
+    x[:, 1] -= 0.0035
+    x += rng.uniform(-3e-4, 3e-4, x.shape)
+    x_all = g.positions(x)
+    targets = x + rng.uniform(-1e-3, 1e-3, x.shape)
+    inertia = sc.mesh.masses * (1 + 1.5 / 60) * 3600
+    eg, gg, hg = g.local_blocks(x_all, 0.008, st, targets=targets, inertia=inertia)
+    eo, go, ho = o.local_blocks(x_all, 0.008, st, targets=targets, inertia=inertia)
+    assert np.all(np.abs(eg - eo) <= BLOCK_RTOL * np.maximum(np.abs(eo), 1e-12))
+    gscale = np.linalg.norm(go, axis=1, keepdims=True) + 1e-12
+    assert np.all(np.abs(gg - go) <= BLOCK_RTOL * gscale + 1e-15)
+    hscale = np.abs(ho).max(axis=(1, 2), keepdims=True) + 1e-12
+    assert np.all(np.abs(hg - ho) <= BLOCK_RTOL * hscale)
+
+
+def test_local_blocks_with_grab_and_default_fabric():
+    sc = scenes.demo_left_panel(3, 4)
+    g = VbdSolver(sc)
+    o = oracle.Solver(sc)
+    rng = np.random.default_rng(1)
+    x = sc.x0 + rng.uniform(-0.01, 0.01, sc.x0.shape)
+    grab = dict(vertices=[0, 5, 6], weights=[0.2, 0.3, 0.5], target=[0.0, 0.9, 0.05], stiffness=100.0)
+    st = sc.settings.to_c()
+    eg, gg, hg = g.local_blocks(x, 0.01, st, grab=grab)
+    eo, go, ho = o.local_blocks(x, 0.01, st, grab=grab)
+    assert np.allclose(eg, eo, rtol=BLOCK_RTOL, atol=1e-15)
+    assert np.allclose(gg, go, rtol=1e-8, atol=1e-12 * np.abs(go).max())
+    assert np.allclose(hg, ho, rtol=1e-8, atol=1e-12 * np.abs(ho).max())
+
+
+def test_coloring_matches_sequential_greedy():
+    sc = contact_scene(20)
+    g = VbdSolver(sc)
+    o = oracle.Solver(sc)
+    x = sc.x0.copy()
+    x[:, 1] -= 0.0037
+    x_all = g.positions(x)
+    grab = dict(vertices=[0, 21, 22], weights=[0.2, 0.3, 0.5], target=[0.0, 0.2, 0.0], stiffness=100.0)
+    for gr in (None, grab):
+        cg, ng = g.colors(x_all, 0.008, sc.settings, grab=gr)
+        co, no = o.colors(x_all, 0.008, sc.settings.ogc_c(), grab=gr)
+        assert ng == no
+        assert np.array_equal(cg, co)
+
+
+@pytest.mark.parametrize("maker", [lambda: scenes.small_sheet(16, seed=2),
+                                   lambda: contact_scene(16, seed=4)])
+def test_one_step_positions_within_1e5_m(maker):
+    sc = maker()
+    # advance a state with the oracle so contact is exercised, then step it
+    # once with two fresh solvers (neither has adaptive-init history)
+    o = oracle.Solver(sc, threads=8)
+    st = sc.settings.to_c()
+    x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
+    for _ in range(3):
+        x, v, t, _ = o.step(x, v, t, st)
+    g = VbdSolver(sc)
+    o2 = oracle.Solver(sc, threads=8)
+    xg, vg, tg, mg = g.step(x, v, t, st)
+    xo, vo, to, mo = o2.step(x, v, t, st)
+    err = np.linalg.norm(xg - xo, axis=1).max()
+    assert err <= POSITION_TOL_M, err
+    assert tg == to
+    assert mg["contact_terms"] == mo["contact_terms"]
+    assert mg["detection_updates"] == mo["detection_updates"]
+
+
+def test_stepping_with_history_stays_within_1e5_m():
+    """Both solvers advance their own trajectories (adaptive-init history
+    active from step 2 on); per-step deviation stays within bar (a)."""
+    sc = contact_scene(16, seed=9)
+    out, _, _ = run_both(sc, 8)
+    for k, (xg, xo, mg, mo) in enumerate(out):
+        err = np.linalg.norm(xg - xo, axis=1).max()
+        assert err <= POSITION_TOL_M, (k, err)
+
+
+def test_config0_one_step_parity():
+    sc = scenes.config0()
+    out, _, _ = run_both(sc, 1)
+    xg, xo, mg, mo = out[0]
+    err = np.linalg.norm(xg - xo, axis=1).max()
+    assert err <= POSITION_TOL_M, err
+    assert mg["contact_terms"] == mo["contact_terms"]
+    assert mg["colors"] == mo["colors"]
+
+
+def test_many_steps_energy_and_residual_within_one_percent():
+    sc = contact_scene(16, seed=6)
+    out, g, o = run_both(sc, 40)
+    xg, xo, mg, mo = out[-1]
+    for key in ("residual_rms_n",):
+        assert abs(mg[key] - mo[key]) <= RELATIVE_TOL * abs(mo[key]) + 1e-12, (mg[key], mo[key])
+    # total potential (membrane + bending + contact) via the oracle's blocks at each final state
+    st = sc.settings.to_c()
+    eg = o.local_blocks(o.positions(xg), 0.008, st)[0].sum()
+    eo = o.local_blocks(o.positions(xo), 0.008, st)[0].sum()
+    assert abs(eg - eo) <= RELATIVE_TOL * abs(eo), (eg, eo)
+
+
+# ---------------------------------------------------- reference known answers
+def test_resting_contact_settles_without_sawtooth_on_gpu():  # tests/vbd.rs:10-34
+    for offset in ((0.0, 0.0, 0.0), (100.0, 101.4, -100.0)):
+        sc = scenes.resting_patch(offset)
+        s = VbdSolver(sc)
+        st = sc.settings.to_c()
+        x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
+        max_delta = 0.0
+        for i in range(60):
+            old = x.copy()
+            x, v, t, _ = s.step(x, v, t, st)
+            assert np.all(np.abs(x[:, 1] - offset[1] - st.contact.radius) < 1e-5), (i, x[:, 1])
+            if i > 10:
+                max_delta = max(max_delta, float(np.abs(x[:, 1] - old[:, 1]).max()))
+        assert max_delta < 1e-6
+
+
+def test_free_fall_matches_backward_euler_on_gpu():  # tests/vbd.rs:44-61
+    sc = scenes.demo_left_panel()
+    s = VbdSolver(sc)
+    st = scenes.StepSettings(dt=0.005, damping=0.0, iterations=3).to_c()
+    x, v, t, _ = s.step(sc.x0, sc.v0, 0.0, st)
+    g = np.array([0.0, -9.81, 0.0])
+    assert np.all(np.linalg.norm(v - g * 0.005, axis=1) < 1e-9)
+    assert np.all(np.linalg.norm(x - sc.x0 - g * 0.005 ** 2, axis=1) < 1e-12)
+
+
+def test_grab_pulls_and_invalid_input_is_transactional_on_gpu():  # tests/vbd.rs:62-91
+    sc = scenes.demo_left_panel()
+    s = VbdSolver(sc)
+    tri = sc.mesh.triangles[0]
+    center = sum(sc.x0[i] / 3.0 for i in tri)
+    grab = dict(vertices=tri, weights=[1 / 3] * 3, target=center + np.array([0, 0, 0.01]), stiffness=100.0)
+    st = scenes.StepSettings(gravity=(0.0, 0.0, 0.0), iterations=6).to_c()
+    x, v, t, _ = s.step(sc.x0, sc.v0, 0.0, st, grab)
+    assert sum(x[i] / 3.0 for i in tri)[2] > center[2]
+    x_before, t_before = x.copy(), t
+    with pytest.raises(VbdError):
+        s.step(x, v, t, st, dict(grab, target=np.array([np.nan, 0, 0])))
+    # the caller's arrays are untouched and the solver still steps
+    assert np.array_equal(x, x_before) and t == t_before
+    s.step(x, v, t, st, grab)
+
+
+def test_invalid_settings_and_state_are_rejected_on_gpu():
+    sc = scenes.demo_left_panel()
+    s = VbdSolver(sc)
+    with pytest.raises(VbdError):
+        s.step(sc.x0, sc.v0, 0.0, scenes.StepSettings(dt=0.1).to_c())
+    v = sc.v0.copy()
+    v[0, 0] = np.inf
+    with pytest.raises(VbdError):
+        s.step(sc.x0, v, 0.0, scenes.StepSettings().to_c())
+
+
+def test_resident_stepping_equals_host_stepping():
+    sc = contact_scene(12, seed=8)
+    st = sc.settings.to_c()
+    a = VbdSolver(sc)
+    b = VbdSolver(sc)
+    x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
+    b.set_state(x, v, t)
+    for _ in range(5):
+        x, v, t, _ = a.step(x, v, t, st)
+        b.step_resident(st)
+    xb, vb, tb = b.get_state()
+    assert np.array_equal(x, xb) and np.array_equal(v, vb) and t == tb
