@@ -104,7 +104,8 @@ class cc_metrics(C.Structure):
             "extension_max_percent", "residual_rms_n")] + [
         ("has_residual", C.c_int32), ("reserved0", C.c_int32),
         ("sweep_ms", C.c_double)] + [(n, C.c_uint64) for n in (
-            "sweep_launches", "vertex_solves", "kernel_launches", "contact_incidence")]
+            "sweep_launches", "vertex_solves", "kernel_launches", "contact_incidence")] + [
+        ("color_ms", C.c_double), ("color_rounds", C.c_uint64)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}

@@ -5,12 +5,11 @@
 // The reference visits vertices 0..n in order and gives each the smallest
 // colour not used by an already-coloured neighbour (material graph, contact
 // co-vertices, grab). Already-coloured means lower index, so the result is
-// the unique solution of  c(v) = mex { c(u) : u ~ v, u < v }.  That system is
-// solved here by Jacobi fixed-point iteration: every vertex re-evaluates its
-// rule from the previous iterate, in parallel. A vertex is final once all its
-// lower neighbours are, so the iteration reaches the exact sequential result
-// in at most (longest descending chain + 1) sweeps; starting from the previous
-// detection's colouring it usually needs far fewer.
+// the unique solution of  c(v) = mex { c(u) : u ~ v, u < v }.  A plain
+// parallel fixed-point iteration of that system needs as many sweeps as the
+// longest descending chain, and contact edges between folded layers make
+// chains of length ~n; k_color_chunked below bounds the work by walking
+// index-ordered chunks instead.
 #include <cub/device/device_scan.cuh>
 
 #include "color.cuh"
@@ -22,52 +21,101 @@ __device__ __forceinline__ void mark(unsigned long long& mask, uint32_t c, bool&
     else high = true;
 }
 
-__global__ void k_color_step(ColorView g, const uint16_t* cin, uint16_t* cout, unsigned int* changed) {
-    unsigned int any = 0;
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x) {
-        unsigned long long mask = 0;
-        bool high = false;
-        for (uint32_t k = g.lo_off[v]; k < g.lo_off[v + 1]; ++k) mark(mask, cin[g.lo[k]], high);
-        for (uint32_t k = g.contacts.inc_off[v]; k < g.contacts.inc_off[v + 1]; ++k) {
+// Greedy rule for one vertex: smallest colour not used by a lower-index
+// neighbour (material graph, contact co-vertices, grab).
+__device__ __forceinline__ uint32_t greedy_color(const ColorView& g, const uint16_t* cin, uint32_t v) {
+    unsigned long long mask = 0;
+    bool high = false;
+    for (uint32_t k = g.lo_off[v]; k < g.lo_off[v + 1]; ++k) mark(mask, cin[g.lo[k]], high);
+    for (uint32_t k = g.contacts.inc_off[v]; k < g.contacts.inc_off[v + 1]; ++k) {
+        uint32_t c = g.contacts.inc[k];
+        uint32_t kind = g.contacts.kind[c];
+        uint4 cv = g.contacts.verts[c];
+        uint32_t ids[4] = {cv.x, cv.y, cv.z, cv.w};
+        uint32_t cnt = kind == 0 ? 2u : (kind == 1 ? 3u : 4u);
+        for (uint32_t j = 0; j < cnt; ++j)
+            if (ids[j] < v) mark(mask, cin[ids[j]], high);
+    }
+    bool in_grab = g.grab_active && (g.grab_v[0] == v || g.grab_v[1] == v || g.grab_v[2] == v);
+    if (in_grab)
+        for (int j = 0; j < 3; ++j)
+            if (g.grab_v[j] < v) mark(mask, cin[g.grab_v[j]], high);
+    if (~mask != 0ull) return (uint32_t)__ffsll((long long)~mask) - 1;
+    for (uint32_t col = 64;; ++col) {  // more than 64 colours around v: linear search
+        bool used = false;
+        for (uint32_t k = g.lo_off[v]; k < g.lo_off[v + 1] && !used; ++k) used = cin[g.lo[k]] == col;
+        for (uint32_t k = g.contacts.inc_off[v]; k < g.contacts.inc_off[v + 1] && !used; ++k) {
             uint32_t c = g.contacts.inc[k];
             uint32_t kind = g.contacts.kind[c];
             uint4 cv = g.contacts.verts[c];
             uint32_t ids[4] = {cv.x, cv.y, cv.z, cv.w};
             uint32_t cnt = kind == 0 ? 2u : (kind == 1 ? 3u : 4u);
-            for (uint32_t j = 0; j < cnt; ++j)
-                if (ids[j] < v) mark(mask, cin[ids[j]], high);
+            for (uint32_t j = 0; j < cnt; ++j) used = used || (ids[j] < v && cin[ids[j]] == col);
         }
-        bool in_grab = g.grab_active && (g.grab_v[0] == v || g.grab_v[1] == v || g.grab_v[2] == v);
         if (in_grab)
-            for (int j = 0; j < 3; ++j)
-                if (g.grab_v[j] < v) mark(mask, cin[g.grab_v[j]], high);
-        uint32_t col;
-        if (~mask != 0ull) {
-            col = (uint32_t)__ffsll((long long)~mask) - 1;
-        } else {
-            // more than 64 colours in the neighbourhood: linear search
-            col = 64;
-            for (;; ++col) {
-                bool used = false;
-                for (uint32_t k = g.lo_off[v]; k < g.lo_off[v + 1] && !used; ++k) used = cin[g.lo[k]] == col;
-                for (uint32_t k = g.contacts.inc_off[v]; k < g.contacts.inc_off[v + 1] && !used; ++k) {
-                    uint32_t c = g.contacts.inc[k];
-                    uint32_t kind = g.contacts.kind[c];
-                    uint4 cv = g.contacts.verts[c];
-                    uint32_t ids[4] = {cv.x, cv.y, cv.z, cv.w};
-                    uint32_t cnt = kind == 0 ? 2u : (kind == 1 ? 3u : 4u);
-                    for (uint32_t j = 0; j < cnt; ++j) used = used || (ids[j] < v && cin[ids[j]] == col);
-                }
-                if (in_grab)
-                    for (int j = 0; j < 3; ++j) used = used || (g.grab_v[j] < v && cin[g.grab_v[j]] == col);
-                if (!used || col >= kMaxColors - 1) break;
-            }
-        }
-        (void)high;
-        if (col != cin[v]) any = 1;
-        cout[v] = (uint16_t)col;
+            for (int j = 0; j < 3; ++j) used = used || (g.grab_v[j] < v && cin[g.grab_v[j]] == col);
+        if (!used || col >= kMaxColors - 1) return col;
     }
-    if (any) atomicOr(changed, 1u);
+}
+
+// Exact sequential-greedy colouring by one CTA: chunks of kChunk consecutive
+// vertices are visited in index order, so every lower neighbour outside the
+// current chunk is already final; inside the chunk the greedy rule is
+// iterated Jacobi-style (read all, barrier, write changes) until no colour
+// changes. A chunk converges in at most (its internal descending chain + 1)
+// rounds <= kChunk + 1, so the loop is bounded; starting from the previous
+// colouring a chunk usually settles in one or two rounds.
+//
+// The walk starts at the chunk of `first[0]`, the lowest vertex whose rule
+// does not hold for the previous colouring (k_color_probe): every vertex
+// below it already satisfies the rule against final lower neighbours, so it
+// is final too. When the whole colouring fits (n <= kSmemColors) it is kept
+// in shared memory for the walk.
+constexpr int kChunk = 1024;
+constexpr uint32_t kSmemColors = 96 * 1024;  // 192 KB of uint16 colours
+__global__ void __launch_bounds__(kChunk) k_color_chunked(ColorView g, uint16_t* col_g, const unsigned int* first,
+                                                         unsigned int* rounds_out, unsigned int* err) {
+    extern __shared__ uint16_t col_s[];
+    uint32_t start = *first;
+    if (start >= g.n) {  // already a fixed point
+        if (threadIdx.x == 0) *rounds_out = 0;
+        return;
+    }
+    bool smem = g.n <= kSmemColors;
+    uint16_t* col = col_g;
+    if (smem) {
+        for (uint32_t i = threadIdx.x; i < g.n; i += kChunk) col_s[i] = col_g[i];
+        __syncthreads();
+        col = col_s;
+    }
+    unsigned int rounds = 0;
+    for (uint32_t base = (start / kChunk) * kChunk; base < g.n; base += kChunk) {
+        uint32_t v = base + threadIdx.x;
+        int r = 0;
+        for (; r <= kChunk + 1; ++r) {
+            uint32_t c = v < g.n ? greedy_color(g, col, v) : 0u;
+            __syncthreads();
+            int changed = (v < g.n && c != col[v]) ? 1 : 0;
+            if (changed) col[v] = (uint16_t)c;
+            ++rounds;
+            if (!__syncthreads_or(changed)) break;
+        }
+        if (r > kChunk + 1 && threadIdx.x == 0) atomicOr(err, 1u);
+    }
+    if (smem) {
+        __syncthreads();
+        for (uint32_t i = (start / kChunk) * kChunk + threadIdx.x; i < g.n; i += kChunk) col_g[i] = col_s[i];
+    }
+    if (threadIdx.x == 0) *rounds_out = rounds;
+}
+
+// Lowest vertex whose greedy rule fails for the current colouring.
+__global__ void k_color_probe(ColorView g, const uint16_t* col, unsigned int* first) {
+    unsigned int lo = 0xffffffffu;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < g.n; v += gridDim.x * blockDim.x)
+        if (greedy_color(g, col, v) != col[v]) lo = min(lo, v);
+    for (int o = 16; o > 0; o >>= 1) lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    if ((threadIdx.x & 31) == 0 && lo != 0xffffffffu) atomicMin(first, lo);
 }
 
 __global__ void k_color_count(uint32_t n, const uint16_t* col, uint32_t* counts) {
@@ -105,38 +153,27 @@ void Coloring::compute(const ColorView& view, cudaStream_t s) {
         offsets_h_.assign(1, 0);
         return;
     }
-    uint16_t* in = cur_;
-    uint16_t* out = (in == a_.ptr) ? b_.ptr : a_.ptr;
-    last_iterations_ = 0;
-    size_t limit = (size_t)n + 2;
-    bool done = false;
-    while (!done) {
-        CC_CUDA(cudaMemsetAsync(changed_.ptr, 0, kBatch * sizeof(unsigned int), s));
-        for (int k = 0; k < kBatch; ++k) {
-            k_color_step<<<grid_for(n, 256), 256, 0, s>>>(view, in, out, changed_.ptr + k);
-            ++launches_;
-            std::swap(in, out);
-        }
-        CC_CUDA(cudaGetLastError());
-        CC_CUDA(cudaMemcpyAsync(changed_h_.ptr, changed_.ptr, kBatch * sizeof(unsigned int), cudaMemcpyDeviceToHost,
-                                s));
-        CC_CUDA(cudaStreamSynchronize(s));
-        for (int k = 0; k < kBatch; ++k) {
-            ++last_iterations_;
-            if (changed_h_.ptr[k] == 0) {
-                done = true;
-                break;
-            }
-        }
-        if (!done && last_iterations_ > limit)
-            throw Failure{CC_ERR_CUDA, "colouring fixed point did not converge"};
-    }
-    cur_ = in;  // the last output (a fixed point: equal to every later iterate)
+    // the chunked walk updates the previous colouring in place, from the
+    // first vertex the probe finds out of date
+    CC_CUDA(cudaMemsetAsync(changed_.ptr, 0, 2 * sizeof(unsigned int), s));
+    CC_CUDA(cudaMemsetAsync(changed_.ptr + 2, 0xff, sizeof(unsigned int), s));
+    k_color_probe<<<grid_for(n, 256), 256, 0, s>>>(view, cur_, changed_.ptr + 2);
+    size_t smem = n <= kSmemColors ? n * sizeof(uint16_t) : 0;
+    if (smem > 48 * 1024 && !smem_attr_)
+        CC_CUDA(cudaFuncSetAttribute(k_color_chunked, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(kSmemColors * sizeof(uint16_t))));
+    smem_attr_ = true;
+    k_color_chunked<<<1, kChunk, smem, s>>>(view, cur_, changed_.ptr + 2, changed_.ptr, changed_.ptr + 1);
+    launches_ += 2;
+    CC_CUDA(cudaGetLastError());
     CC_CUDA(cudaMemsetAsync(counts_.ptr, 0, kMaxColors * sizeof(uint32_t), s));
     CC_CUDA(cudaMemsetAsync(cursor_.ptr, 0, kMaxColors * sizeof(uint32_t), s));
     k_color_count<<<grid_for(n, 256), 256, 0, s>>>(n, cur_, counts_.ptr);
     CC_CUDA(cudaMemcpyAsync(counts_h_.ptr, counts_.ptr, kMaxColors * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    CC_CUDA(cudaMemcpyAsync(changed_h_.ptr, changed_.ptr, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     CC_CUDA(cudaStreamSynchronize(s));
+    last_iterations_ = changed_h_.ptr[0];
+    if (changed_h_.ptr[1]) throw Failure{CC_ERR_CUDA, "colouring rounds exceeded their bound"};
     n_colors_ = 0;
     for (uint32_t c = 0; c < kMaxColors; ++c)
         if (counts_h_.ptr[c]) n_colors_ = c + 1;

@@ -55,8 +55,12 @@ struct DBuf {
         cap = 0;
     }
     // Ensure room for n elements; contents are not preserved on growth.
+    // Growth is geometric (x1.5) so that buffers sized by data-dependent
+    // counts (contacts, pairs) reallocate - and synchronise - rarely.
     void reserve(size_t n) {
         if (n <= cap) return;
+        size_t grown = cap + cap / 2;
+        if (cap && grown > n) n = grown;
         release();
         size_t bytes = (n ? n : 1) * sizeof(T);
         CC_CUDA(cudaMalloc(&ptr, bytes));

@@ -264,6 +264,9 @@ struct cc_solver {
     std::vector<cudaEvent_t> prof_events;
     uint64_t own_launches = 0;
     uint32_t n_free = 0;
+    int lanes = 0;          // vertices are solved by groups of `lanes` threads; 0 = autotune on next step
+    DBuf<double4> x_backup;
+    std::vector<double> tune_ms;
     std::string err;
     int code = 0;
     int fail(const Failure& f) {
@@ -345,7 +348,49 @@ struct cc_solver {
     }
 
     void step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out);
+    void autotune(const SweepView& sv);
+    void color(const ContactsView& cv, const cc_grab* grab, cc_metrics& m) {
+        double t = now_ms();
+        coloring.compute(color_view(cv, grab), stream);
+        m.color_ms += now_ms() - t;
+        m.color_rounds += coloring.last_iterations();
+    }
 };
+
+// Project autotuner: time one full colour sweep per candidate group width on
+// a backup of the positions (restored after each trial) and keep the fastest.
+void cc_solver::autotune(const SweepView& sv) {
+    static const int kCandidates[] = {1, 2, 4, 8, 16, 32};
+    x_backup.reserve(n);
+    CC_CUDA(cudaMemcpyAsync(x_backup.ptr, world->x(), n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
+    const auto& off = coloring.offsets();
+    tune_ms.clear();
+    float best = 1e30f;
+    int best_g = 8;
+    for (int g : kCandidates) {
+        float total = 1e30f;
+        for (int rep = 0; rep < 4; ++rep) {  // first repetition warms caches; keep the fastest of the rest
+            CC_CUDA(cudaEventRecord(ev0, stream));
+            for (uint32_t c = 0; c < coloring.n_colors(); ++c)
+                launch_sweep(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
+            CC_CUDA(cudaEventRecord(ev1, stream));
+            CC_CUDA(cudaMemcpyAsync(world->x(), x_backup.ptr, n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
+            CC_CUDA(cudaEventSynchronize(ev1));
+            CC_CUDA(cudaGetLastError());
+            float t = 0.f;
+            CC_CUDA(cudaEventElapsedTime(&t, ev0, ev1));
+            if (rep > 0) total = std::min(total, t);
+            own_launches += coloring.n_colors();
+        }
+        tune_ms.push_back(total);
+        if (total < best) {
+            best = total;
+            best_g = g;
+        }
+    }
+    CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
+    lanes = best_g;
+}
 
 void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out) {
     if (!vbd_valid(s)) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid VBD settings"};
@@ -394,7 +439,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     }
     if (md <= 1e-12) throw Failure{CC_ERR_CONTACT, "OGC zero separation; step rejected, reset the arrangement"};
     ContactsView cv = world->contacts();
-    coloring.compute(color_view(cv, grab), stream);
+    color(cv, grab, m);
     CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
     k_warm_start<<<gb, 256, 0, stream>>>(n, pinned.ptr, guess.ptr, cv, world->x(), sc.ptr);
     ++own_launches;
@@ -405,10 +450,11 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         if (clipped > 0 && (double)clipped >= s.contact.refresh_fraction * (double)n) {
             detect(rq, s.contact, &m, det_ms);
             cv = world->contacts();
-            coloring.compute(color_view(cv, grab), stream);
+            color(cv, grab, m);
         }
-        CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
         SweepView sv = sweep_view(cv, s, grab);
+        if (lanes == 0) autotune(sv);
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
         const auto& off = coloring.offsets();
         for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
             uint32_t cnt = off[c + 1] - off[c];
@@ -421,7 +467,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                 }
                 CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
             }
-            launch_sweep(sv, coloring.order() + off[c], cnt, 1, stream);
+            launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
             if (profiling) {
                 CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
                 prof_used += 2;
@@ -767,6 +813,13 @@ int32_t cc_solver_set_profiling(cc_solver* s, int32_t enable) {
     s->profiling = enable != 0;
     return CC_OK;
 }
+int32_t cc_solver_set_lanes(cc_solver* s, int32_t lanes) {
+    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32))
+        return s->fail(Failure{CC_ERR_INVALID_ARGUMENT, "lanes must be 0 (autotune) or a power of two up to 32"});
+    s->lanes = lanes;
+    return CC_OK;
+}
+int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes; }
 cc_world* cc_solver_world(cc_solver* s) { return &s->world_view; }
 
 static void upload_state(cc_solver* s, const double* x, const double* v) {

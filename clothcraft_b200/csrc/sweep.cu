@@ -8,6 +8,13 @@
 // decrease (src/vbd.rs:353-386). The reference GPU shader uses Gauss-Newton
 // Hessians and 8 halvings; this kernel follows the CPU path instead.
 //
+// A group of G lanes (G in 1..32, chosen per workload) solves one vertex: the
+// incident terms are dealt round-robin to the lanes, each lane accumulates a
+// partial energy / gradient / Hessian, and a butterfly shuffle reduction gives
+// every lane of the group the same bitwise total (each level adds the same two
+// partial sums, and addition is commutative), so all lanes take identical
+// line-search decisions without a broadcast.
+//
 // All arithmetic is FP64: at cloth resolutions the in-plane membrane
 // stiffness per vertex (~1e5 N/m) is six to seven orders above the inertia
 // term (m/dt^2 ~ 1e-2 N/m), so an FP32 Hessian cannot represent the soft
@@ -32,27 +39,18 @@ __device__ __forceinline__ void sym_add_outer(Sym& h, d3 u, double s) {  // h +=
     h.a[4] += s * u.y * u.z;
     h.a[5] += s * u.z * u.z;
 }
+__device__ __forceinline__ void sym_add_outer2(Sym& h, d3 u, d3 v, double s) {  // h += s (u v^T + v u^T)
+    h.a[0] += s * 2.0 * u.x * v.x;
+    h.a[1] += s * (u.x * v.y + v.x * u.y);
+    h.a[2] += s * (u.x * v.z + v.x * u.z);
+    h.a[3] += s * 2.0 * u.y * v.y;
+    h.a[4] += s * (u.y * v.z + v.y * u.z);
+    h.a[5] += s * 2.0 * u.z * v.z;
+}
 __device__ __forceinline__ void sym_add_diag(Sym& h, double s) {
     h.a[0] += s;
     h.a[3] += s;
     h.a[5] += s;
-}
-
-struct M33 {
-    double m[3][3];  // row-major
-};
-__device__ __forceinline__ M33 skew(d3 v) {  // [v]x : a -> v x a
-    M33 r;
-    r.m[0][0] = 0.0;
-    r.m[0][1] = -v.z;
-    r.m[0][2] = v.y;
-    r.m[1][0] = v.z;
-    r.m[1][1] = 0.0;
-    r.m[1][2] = -v.x;
-    r.m[2][0] = -v.y;
-    r.m[2][1] = v.x;
-    r.m[2][2] = 0.0;
-    return r;
 }
 
 // ----------------------------------------------------------------- terms
@@ -65,6 +63,11 @@ __device__ __forceinline__ void axial3(double s, double k, double c, double delt
     double p2 = 0.5 * delta * delta / (r * r * r);
     f1 = k * (c * s + (1.0 - c) * p * p1);
     f2 = k * (c + (1.0 - c) * (p1 * p1 + p * p2));
+}
+__device__ __forceinline__ double axial1(double s, double k, double c, double delta) {
+    double r = sqrt(s * s + delta * delta);
+    double p = (s + r - delta) * 0.5;
+    return 0.5 * k * (c * s * s + (1.0 - c) * p * p);
 }
 
 __device__ __forceinline__ d3 pos(const SweepView& s, uint32_t i, uint32_t v, d3 p) {
@@ -87,28 +90,48 @@ __device__ __forceinline__ double membrane_term(const SweepView& s, uint32_t t, 
     double ew = (dot(w, w) - 1.0) * 0.5;
     double ev = (dot(v, v) - 1.0) * 0.5;
     double sh = dot(w, v);
+    if (!D) return A * (axial1(ew, M.warp, M.c, M.delta) + axial1(ev, M.weft, M.c, M.delta) + 0.5 * M.shear * sh * sh);
     double fw, fw1, fw2, fv, fv1, fv2;
     axial3(ew, M.warp, M.c, M.delta, fw, fw1, fw2);
     axial3(ev, M.weft, M.c, M.delta, fv, fv1, fv2);
-    double e = A * (fw + fv + 0.5 * M.shear * sh * sh);
-    if (D) {
-        double aw = slot == 0 ? -(cf.x + cf.y) : (slot == 1 ? cf.x : cf.y);
-        double av = slot == 0 ? -(cf.z + cf.w) : (slot == 1 ? cf.z : cf.w);
-        d3 q = v * aw + w * av;
-        g = g + (w * (fw1 * aw) + v * (fv1 * av) + q * (M.shear * sh)) * A;
-        sym_add_outer(H, w, A * fw2 * aw * aw);
-        sym_add_outer(H, v, A * fv2 * av * av);
-        sym_add_outer(H, q, A * M.shear);
-        sym_add_diag(H, A * (fw1 * aw * aw + fv1 * av * av + 2.0 * M.shear * sh * aw * av));
-    }
-    return e;
+    double aw = slot == 0 ? -(cf.x + cf.y) : (slot == 1 ? cf.x : cf.y);
+    double av = slot == 0 ? -(cf.z + cf.w) : (slot == 1 ? cf.z : cf.w);
+    d3 q = v * aw + w * av;
+    g = g + (w * (fw1 * aw) + v * (fv1 * av) + q * (M.shear * sh)) * A;
+    sym_add_outer(H, w, A * fw2 * aw * aw);
+    sym_add_outer(H, v, A * fv2 * av * av);
+    sym_add_outer(H, q, A * M.shear);
+    sym_add_diag(H, A * (fw1 * aw * aw + fv1 * av * av + 2.0 * M.shear * sh * aw * av));
+    return A * (fw + fv + 0.5 * M.shear * sh * sh);
+}
+
+// P_k [a]x / l as three columns: P(a x e_j)/l, P y = y - h (h.y)
+__device__ __forceinline__ void proj_skew_cols(d3 a, d3 h, double inv_l, double sign, d3& c0, d3& c1, d3& c2) {
+    d3 e0 = mk(0.0, a.z, -a.y), e1 = mk(-a.z, 0.0, a.x), e2 = mk(a.y, -a.x, 0.0);
+    double f = sign * inv_l;
+    c0 = c0 + (e0 - h * dot(h, e0)) * f;
+    c1 = c1 + (e1 - h * dot(h, e1)) * f;
+    c2 = c2 + (e2 - h * dot(h, e2)) * f;
+}
+
+// [a]x^T M [a]x for M = -(1/l^2)[d h^T + h d^T + (d.h)(I - 3 h h^T)]
+__device__ __forceinline__ void add_curvature(Sym& Hm, d3 a, d3 h, d3 d, double inv_l2, double sign) {
+    d3 da = cross(d, a), ha = cross(h, a);
+    double dh = dot(d, h);
+    double sc = -inv_l2 * sign;
+    sym_add_outer2(Hm, da, ha, sc);
+    double aa = dot(a, a);
+    sym_add_diag(Hm, sc * dh * aa);
+    sym_add_outer(Hm, a, -sc * dh);
+    sym_add_outer(Hm, ha, -3.0 * sc * dh);
 }
 
 // bending (src/energy.rs:31-46) of hinge h with vertex slot `slot` at p.
+// n1 = e x u, n2 = w x e are affine in one vertex: dn_k/dp = [a_k]x.
 template <bool D>
-__device__ __forceinline__ double bending_term(const SweepView& s, uint32_t h, uint32_t slot, d3 p, d3& g, Sym& H) {
-    uint4 hv = s.hinge_v[h];
-    double K = s.hinge_k[h];
+__device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, uint32_t slot, d3 p, d3& g, Sym& H) {
+    uint4 hv = s.hinge_v[hi];
+    double K = s.hinge_k[hi];
     d3 x0 = slot == 0 ? p : ld3(s.x, hv.x);
     d3 x1 = slot == 1 ? p : ld3(s.x, hv.y);
     d3 x2 = slot == 2 ? p : ld3(s.x, hv.z);
@@ -121,72 +144,30 @@ __device__ __forceinline__ double bending_term(const SweepView& s, uint32_t h, u
     d3 h1 = n1 / l1, h2 = n2 / l2;
     d3 d = h1 - h2;
     double energy = K * dot(d, d);
-    if (D) {
-        // dn/dp as cross-product matrices (n1, n2 are affine in one vertex)
-        M33 A1, A2;
-        bool has1 = slot != 3, has2 = slot != 2;
-        if (slot == 0) {
-            A1 = skew(u - e);
-            A2 = skew(e - w);
-        } else if (slot == 1) {
-            A1 = skew(-u);
-            A2 = skew(w);
-        } else if (slot == 2) {
-            A1 = skew(e);
-        } else {
-            A2 = skew(-e);
-        }
-        // J_k = (I - h h^T) A_k / l_k ; J = J1 - J2
-        double J[3][3];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) J[i][j] = 0.0;
-        double hh1[3] = {h1.x, h1.y, h1.z}, hh2[3] = {h2.x, h2.y, h2.z}, dd[3] = {d.x, d.y, d.z};
-        if (has1) {
-            for (int j = 0; j < 3; ++j) {
-                double hA = hh1[0] * A1.m[0][j] + hh1[1] * A1.m[1][j] + hh1[2] * A1.m[2][j];
-                for (int i = 0; i < 3; ++i) J[i][j] += (A1.m[i][j] - hh1[i] * hA) / l1;
-            }
-        }
-        if (has2) {
-            for (int j = 0; j < 3; ++j) {
-                double hA = hh2[0] * A2.m[0][j] + hh2[1] * A2.m[1][j] + hh2[2] * A2.m[2][j];
-                for (int i = 0; i < 3; ++i) J[i][j] -= (A2.m[i][j] - hh2[i] * hA) / l2;
-            }
-        }
-        double gg[3];
-        for (int j = 0; j < 3; ++j) gg[j] = 2.0 * K * (J[0][j] * dd[0] + J[1][j] * dd[1] + J[2][j] * dd[2]);
-        g = g + mk(gg[0], gg[1], gg[2]);
-        double Hm[3][3];
-        for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) Hm[a][b] = J[0][a] * J[0][b] + J[1][a] * J[1][b] + J[2][a] * J[2][b];
-        // + A^T M A with M = -(1/l^2)[d h^T + h d^T + (d.h)(I - 3 h h^T)], sign - for n2
-        for (int k = 0; k < 2; ++k) {
-            if ((k == 0 && !has1) || (k == 1 && !has2)) continue;
-            const M33& A = k == 0 ? A1 : A2;
-            const double* hk = k == 0 ? hh1 : hh2;
-            double l = k == 0 ? l1 : l2;
-            double dh = dd[0] * hk[0] + dd[1] * hk[1] + dd[2] * hk[2];
-            double M[3][3];
-            double sc = -1.0 / (l * l);
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j)
-                    M[i][j] = sc * (dd[i] * hk[j] + hk[i] * dd[j] + dh * ((i == j ? 1.0 : 0.0) - 3.0 * hk[i] * hk[j]));
-            double MA[3][3];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) MA[i][j] = M[i][0] * A.m[0][j] + M[i][1] * A.m[1][j] + M[i][2] * A.m[2][j];
-            double sign = k == 0 ? 1.0 : -1.0;
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b)
-                    Hm[a][b] += sign * (A.m[0][a] * MA[0][b] + A.m[1][a] * MA[1][b] + A.m[2][a] * MA[2][b]);
-        }
-        double f = 2.0 * K;
-        H.a[0] += f * Hm[0][0];
-        H.a[1] += f * 0.5 * (Hm[0][1] + Hm[1][0]);
-        H.a[2] += f * 0.5 * (Hm[0][2] + Hm[2][0]);
-        H.a[3] += f * Hm[1][1];
-        H.a[4] += f * 0.5 * (Hm[1][2] + Hm[2][1]);
-        H.a[5] += f * Hm[2][2];
-    }
+    if (!D) return energy;
+    d3 a1 = slot == 0 ? u - e : (slot == 1 ? -u : (slot == 2 ? e : mk(0, 0, 0)));
+    d3 a2 = slot == 0 ? e - w : (slot == 1 ? w : (slot == 3 ? -e : mk(0, 0, 0)));
+    double il1 = 1.0 / l1, il2 = 1.0 / l2;
+    // gradient 2K J^T d with J^T d = sum_k s_k ((P_k d) x a_k) / l_k
+    d3 pd1 = d - h1 * dot(h1, d), pd2 = d - h2 * dot(h2, d);
+    d3 jtd = cross(pd1, a1) * il1 - cross(pd2, a2) * il2;
+    g = g + jtd * (2.0 * K);
+    // Hessian 2K [J^T J + A1^T M1 A1 - A2^T M2 A2]
+    d3 c0 = mk(0, 0, 0), c1 = mk(0, 0, 0), c2 = mk(0, 0, 0);
+    proj_skew_cols(a1, h1, il1, 1.0, c0, c1, c2);
+    proj_skew_cols(a2, h2, il2, -1.0, c0, c1, c2);
+    Sym Hm;
+    Hm.a[0] = dot(c0, c0);
+    Hm.a[1] = dot(c0, c1);
+    Hm.a[2] = dot(c0, c2);
+    Hm.a[3] = dot(c1, c1);
+    Hm.a[4] = dot(c1, c2);
+    Hm.a[5] = dot(c2, c2);
+    add_curvature(Hm, a1, h1, d, il1 * il1, 1.0);
+    add_curvature(Hm, a2, h2, d, il2 * il2, -1.0);
+    double f = 2.0 * K;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) H.a[k] += f * Hm.a[k];
     return energy;
 }
 
@@ -202,94 +183,71 @@ __device__ __forceinline__ double stitch_term(const SweepView& s, uint32_t st, u
         if (j == v) wv += w;
     }
     double K = s.st_k[st];
-    double e = 0.5 * K * dot(d, d);
     if (D) {
         g = g + d * (K * wv);
         sym_add_diag(H, K * wv * wv);
     }
-    return e;
+    return 0.5 * K * dot(d, d);
 }
 
 // ----------------------------------------------- contact: forward-mode AD
-// Jet3 with a symmetric Hessian: the same second-order chain rules as
+// Jet3 with a symmetric Hessian: the second-order chain rules of
 // src/math.rs:46-122, restricted to one vertex's three coordinates.
 struct J3 {
     double v;
-    double g[3];
-    double h[6];
+    double g0, g1, g2;
+    double h00, h01, h02, h11, h12, h22;
 };
-__device__ __forceinline__ J3 jc(double v) {
-    J3 r;
-    r.v = v;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.g[i] = 0.0;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) r.h[i] = 0.0;
-    return r;
-}
-__device__ __forceinline__ J3 jvar(double v, int i) {
-    J3 r = jc(v);
-    r.g[i] = 1.0;
-    return r;
-}
+__device__ __forceinline__ J3 jc(double v) { return {v, 0, 0, 0, 0, 0, 0, 0, 0, 0}; }
 __device__ __forceinline__ J3 operator+(const J3& a, const J3& b) {
-    J3 r;
-    r.v = a.v + b.v;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] + b.g[i];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) r.h[i] = a.h[i] + b.h[i];
-    return r;
+    return {a.v + b.v,     a.g0 + b.g0,   a.g1 + b.g1,   a.g2 + b.g2,   a.h00 + b.h00,
+            a.h01 + b.h01, a.h02 + b.h02, a.h11 + b.h11, a.h12 + b.h12, a.h22 + b.h22};
 }
 __device__ __forceinline__ J3 operator-(const J3& a, const J3& b) {
-    J3 r;
-    r.v = a.v - b.v;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] - b.g[i];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) r.h[i] = a.h[i] - b.h[i];
-    return r;
+    return {a.v - b.v,     a.g0 - b.g0,   a.g1 - b.g1,   a.g2 - b.g2,   a.h00 - b.h00,
+            a.h01 - b.h01, a.h02 - b.h02, a.h11 - b.h11, a.h12 - b.h12, a.h22 - b.h22};
 }
 __device__ __forceinline__ J3 operator-(const J3& a) {
-    J3 r;
-    r.v = -a.v;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.g[i] = -a.g[i];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) r.h[i] = -a.h[i];
-    return r;
+    return {-a.v, -a.g0, -a.g1, -a.g2, -a.h00, -a.h01, -a.h02, -a.h11, -a.h12, -a.h22};
 }
-__device__ __constant__ int kSymI[6] = {0, 0, 0, 1, 1, 2};
-__device__ __constant__ int kSymJ[6] = {0, 1, 2, 1, 2, 2};
 __device__ __forceinline__ J3 operator*(const J3& a, const J3& b) {
     J3 r;
     r.v = a.v * b.v;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.g[i] = a.g[i] * b.v + a.v * b.g[i];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        int i = kSymI[k], j = kSymJ[k];
-        r.h[k] = a.h[k] * b.v + a.v * b.h[k] + a.g[i] * b.g[j] + b.g[i] * a.g[j];
-    }
+    r.g0 = a.g0 * b.v + a.v * b.g0;
+    r.g1 = a.g1 * b.v + a.v * b.g1;
+    r.g2 = a.g2 * b.v + a.v * b.g2;
+    r.h00 = a.h00 * b.v + a.v * b.h00 + 2.0 * a.g0 * b.g0;
+    r.h01 = a.h01 * b.v + a.v * b.h01 + a.g0 * b.g1 + b.g0 * a.g1;
+    r.h02 = a.h02 * b.v + a.v * b.h02 + a.g0 * b.g2 + b.g0 * a.g2;
+    r.h11 = a.h11 * b.v + a.v * b.h11 + 2.0 * a.g1 * b.g1;
+    r.h12 = a.h12 * b.v + a.v * b.h12 + a.g1 * b.g2 + b.g1 * a.g2;
+    r.h22 = a.h22 * b.v + a.v * b.h22 + 2.0 * a.g2 * b.g2;
     return r;
 }
-__device__ __forceinline__ J3 chain(const J3& a, double value, double first, double second) {
+__device__ __forceinline__ J3 chain(const J3& a, double value, double f1, double f2) {
     J3 r;
     r.v = value;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) r.g[i] = first * a.g[i];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) r.h[k] = first * a.h[k] + second * a.g[kSymI[k]] * a.g[kSymJ[k]];
+    r.g0 = f1 * a.g0;
+    r.g1 = f1 * a.g1;
+    r.g2 = f1 * a.g2;
+    r.h00 = f1 * a.h00 + f2 * a.g0 * a.g0;
+    r.h01 = f1 * a.h01 + f2 * a.g0 * a.g1;
+    r.h02 = f1 * a.h02 + f2 * a.g0 * a.g2;
+    r.h11 = f1 * a.h11 + f2 * a.g1 * a.g1;
+    r.h12 = f1 * a.h12 + f2 * a.g1 * a.g2;
+    r.h22 = f1 * a.h22 + f2 * a.g2 * a.g2;
     return r;
 }
 __device__ __forceinline__ J3 operator/(const J3& a, const J3& b) {
     return a * chain(b, 1.0 / b.v, -1.0 / (b.v * b.v), 2.0 / (b.v * b.v * b.v));
 }
-__device__ __forceinline__ J3 jsqrt(const J3& a) {
+__device__ __forceinline__ J3 ssqrt(const J3& a) {
     double r = sqrt(a.v);
     return chain(a, r, 0.5 / r, -0.25 / (r * r * r));
 }
-__device__ __forceinline__ J3 jln(const J3& a) { return chain(a, log(a.v), 1.0 / a.v, -1.0 / (a.v * a.v)); }
+__device__ __forceinline__ J3 sln(const J3& a) { return chain(a, log(a.v), 1.0 / a.v, -1.0 / (a.v * a.v)); }
+__device__ __forceinline__ double ssqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ double sln(double x) { return log(x); }
 __device__ __forceinline__ double sval(double x) { return x; }
 __device__ __forceinline__ double sval(const J3& x) { return x.v; }
 template <class S>
@@ -302,10 +260,6 @@ template <>
 __device__ __forceinline__ J3 scst<J3>(double v) {
     return jc(v);
 }
-__device__ __forceinline__ double ssqrt(double x) { return sqrt(x); }
-__device__ __forceinline__ J3 ssqrt(const J3& x) { return jsqrt(x); }
-__device__ __forceinline__ double sln(double x) { return log(x); }
-__device__ __forceinline__ J3 sln(const J3& x) { return jln(x); }
 
 template <class S>
 struct V {
@@ -337,36 +291,136 @@ __device__ __forceinline__ S activation(const S& d, double r, double k) {
     return scst<S>(0.5 * k * tau * tau) - scst<S>(k * tau * tau) * sln(d / scst<S>(tau));
 }
 
-// Contact::energy (src/ogc/potential.rs:39-65)
+// Contact::energy (src/ogc/potential.rs:39-65) on four named points.
 template <class S>
-__device__ __forceinline__ S contact_energy_t(uint32_t kind, double eps, const V<S> p[4], double r, double k) {
+__device__ __forceinline__ S contact_energy_t(uint32_t kind, double eps, const V<S>& p0, const V<S>& p1,
+                                              const V<S>& p2, const V<S>& p3, double r, double k) {
     S d;
     if (kind == 0) {
-        V<S> v = vsub(p[0], p[1]);
+        V<S> v = vsub(p0, p1);
         d = ssqrt(vdot(v, v));
     } else if (kind == 1) {
-        V<S> u = vsub(p[2], p[1]);
-        V<S> w = vsub(p[0], p[1]);
+        V<S> u = vsub(p2, p1);
+        V<S> w = vsub(p0, p1);
         S q = vdot(w, u) / vdot(u, u);
         V<S> dd = {w.x - q * u.x, w.y - q * u.y, w.z - q * u.z};
         d = ssqrt(vdot(dd, dd));
     } else if (kind == 2) {
-        V<S> n = vcross(vsub(p[2], p[1]), vsub(p[3], p[1]));
-        S h = vdot(vsub(p[0], p[1]), n) / ssqrt(vdot(n, n));
+        V<S> n = vcross(vsub(p2, p1), vsub(p3, p1));
+        S h = vdot(vsub(p0, p1), n) / ssqrt(vdot(n, n));
         d = sval(h) < 0.0 ? -h : h;
     } else {
-        V<S> n = vcross(vsub(p[1], p[0]), vsub(p[3], p[2]));
+        V<S> n = vcross(vsub(p1, p0), vsub(p3, p2));
         if (sval(vdot(n, n)) < 1e-30) return scst<S>(0.0);
-        S h = vdot(vsub(p[0], p[2]), n) / ssqrt(vdot(n, n));
+        S h = vdot(vsub(p0, p2), n) / ssqrt(vdot(n, n));
         d = sval(h) < 0.0 ? -h : h;
     }
     S e = activation(d, r, k);
     if (kind == 3) {
-        V<S> n = vcross(vsub(p[1], p[0]), vsub(p[3], p[2]));
+        V<S> n = vcross(vsub(p1, p0), vsub(p3, p2));
         S q = vdot(n, n) / scst<S>(eps);
         if (sval(q) < 1.0) e = e * q * (scst<S>(2.0) - q);
     }
     return e;
+}
+
+// ---- mixed Jet/constant arithmetic: only the moving vertex carries derivatives
+__device__ __forceinline__ J3 operator+(const J3& a, double b) {
+    J3 r = a;
+    r.v += b;
+    return r;
+}
+__device__ __forceinline__ J3 operator+(double a, const J3& b) { return b + a; }
+__device__ __forceinline__ J3 operator-(const J3& a, double b) {
+    J3 r = a;
+    r.v -= b;
+    return r;
+}
+__device__ __forceinline__ J3 operator-(double a, const J3& b) {
+    J3 r = -b;
+    r.v += a;
+    return r;
+}
+__device__ __forceinline__ J3 operator*(const J3& a, double b) {
+    return {a.v * b, a.g0 * b, a.g1 * b, a.g2 * b, a.h00 * b, a.h01 * b, a.h02 * b, a.h11 * b, a.h12 * b, a.h22 * b};
+}
+__device__ __forceinline__ J3 operator*(double a, const J3& b) { return b * a; }
+__device__ __forceinline__ J3 operator/(const J3& a, double b) { return a * (1.0 / b); }
+__device__ __forceinline__ J3 operator/(double a, const J3& b) {
+    return chain(b, 1.0 / b.v, -1.0 / (b.v * b.v), 2.0 / (b.v * b.v * b.v)) * a;
+}
+__device__ __forceinline__ J3 to_j3(const J3& a) { return a; }
+__device__ __forceinline__ J3 to_j3(double a) { return jc(a); }
+
+template <class A, class B>
+struct Pro {
+    using T = J3;
+};
+template <>
+struct Pro<double, double> {
+    using T = double;
+};
+template <class A, class B>
+__device__ __forceinline__ V<typename Pro<A, B>::T> msub(const V<A>& a, const V<B>& b) {
+    return {a.x - b.x, a.y - b.y, a.z - b.z};
+}
+template <class A, class B>
+__device__ __forceinline__ typename Pro<A, B>::T mdot(const V<A>& a, const V<B>& b) {
+    return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <class A, class B>
+__device__ __forceinline__ V<typename Pro<A, B>::T> mcross(const V<A>& a, const V<B>& b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Contact::energy (src/ogc/potential.rs:39-65) with per-point types.
+template <class S0, class S1, class S2, class S3>
+__device__ __forceinline__ J3 contact_jet(uint32_t kind, double eps, const V<S0>& p0, const V<S1>& p1,
+                                          const V<S2>& p2, const V<S3>& p3, double r, double k) {
+    if (kind == 0) {
+        auto v = msub(p0, p1);
+        return to_j3(activation(ssqrt(mdot(v, v)), r, k));
+    }
+    if (kind == 1) {
+        auto u = msub(p2, p1);
+        auto w = msub(p0, p1);
+        auto q = mdot(w, u) / mdot(u, u);
+        auto dx = w.x - q * u.x;
+        auto dy = w.y - q * u.y;
+        auto dz = w.z - q * u.z;
+        return to_j3(activation(ssqrt(dx * dx + dy * dy + dz * dz), r, k));
+    }
+    if (kind == 2) {
+        auto n = mcross(msub(p2, p1), msub(p3, p1));
+        auto h = mdot(msub(p0, p1), n) / ssqrt(mdot(n, n));
+        auto d = sval(h) < 0.0 ? -h : h;
+        return to_j3(activation(d, r, k));
+    }
+    auto n = mcross(msub(p1, p0), msub(p3, p2));
+    auto nn = mdot(n, n);
+    if (sval(nn) < 1e-30) return jc(0.0);
+    auto h = mdot(msub(p0, p2), n) / ssqrt(nn);
+    auto d = sval(h) < 0.0 ? -h : h;
+    J3 e = to_j3(activation(d, r, k));
+    J3 q = to_j3(nn / eps);
+    if (q.v < 1.0) e = e * q * (2.0 - q);
+    return e;
+}
+
+__device__ __forceinline__ V<J3> var_point(d3 p) {
+    J3 a = jc(p.x), b = jc(p.y), c = jc(p.z);
+    a.g0 = 1.0;
+    b.g1 = 1.0;
+    c.g2 = 1.0;
+    return {a, b, c};
+}
+__device__ __forceinline__ V<double> cst_point(const SweepView& s, uint32_t id) {
+    d3 x = ld3(s.x, id);
+    return {x.x, x.y, x.z};
+}
+__device__ __forceinline__ V<double> dpoint(const SweepView& s, uint32_t id, uint32_t v, d3 p) {
+    d3 x = pos(s, id, v, p);
+    return {x.x, x.y, x.z};
 }
 
 template <bool D>
@@ -374,30 +428,31 @@ __device__ __forceinline__ double contact_term(const SweepView& s, uint32_t c, u
     uint32_t kind = s.contacts.kind[c];
     uint4 cv = s.contacts.verts[c];
     double eps = s.contacts.eps[c];
-    uint32_t ids[4] = {cv.x, cv.y, cv.z, cv.w};
     if (D) {
-        V<J3> q[4];
-        for (int k = 0; k < 4; ++k) {
-            if (ids[k] == v) {
-                q[k] = {jvar(p.x, 0), jvar(p.y, 1), jvar(p.z, 2)};
-            } else {
-                d3 x = ld3(s.x, ids[k]);
-                q[k] = {jc(x.x), jc(x.y), jc(x.z)};
-            }
-        }
-        J3 e = contact_energy_t<J3>(kind, eps, q, s.contact_r, s.contact_k);
-        g = g + mk(e.g[0], e.g[1], e.g[2]);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) H.a[k] += e.h[k];
+        // the moving vertex's slot among the used ones (unused slots hold 0)
+        uint32_t cnt = kind == 0 ? 2u : (kind == 1 ? 3u : 4u);
+        int slot = cv.x == v ? 0 : (cv.y == v ? 1 : ((cnt > 2 && cv.z == v) ? 2 : 3));
+        double r = s.contact_r, k = s.contact_k;
+        J3 e;
+        if (slot == 0)
+            e = contact_jet(kind, eps, var_point(p), cst_point(s, cv.y), cst_point(s, cv.z), cst_point(s, cv.w), r, k);
+        else if (slot == 1)
+            e = contact_jet(kind, eps, cst_point(s, cv.x), var_point(p), cst_point(s, cv.z), cst_point(s, cv.w), r, k);
+        else if (slot == 2)
+            e = contact_jet(kind, eps, cst_point(s, cv.x), cst_point(s, cv.y), var_point(p), cst_point(s, cv.w), r, k);
+        else
+            e = contact_jet(kind, eps, cst_point(s, cv.x), cst_point(s, cv.y), cst_point(s, cv.z), var_point(p), r, k);
+        g = g + mk(e.g0, e.g1, e.g2);
+        H.a[0] += e.h00;
+        H.a[1] += e.h01;
+        H.a[2] += e.h02;
+        H.a[3] += e.h11;
+        H.a[4] += e.h12;
+        H.a[5] += e.h22;
         return e.v;
-    } else {
-        V<double> q[4];
-        for (int k = 0; k < 4; ++k) {
-            d3 x = pos(s, ids[k], v, p);
-            q[k] = {x.x, x.y, x.z};
-        }
-        return contact_energy_t<double>(kind, eps, q, s.contact_r, s.contact_k);
     }
+    return contact_energy_t<double>(kind, eps, dpoint(s, cv.x, v, p), dpoint(s, cv.y, v, p), dpoint(s, cv.z, v, p),
+                                    dpoint(s, cv.w, v, p), s.contact_r, s.contact_k);
 }
 
 // grab 0.5 k |sum w_j x_j - target|^2 (src/vbd.rs:237-246)
@@ -406,33 +461,43 @@ __device__ __forceinline__ double grab_term(const SweepView& s, uint32_t v, d3 p
     const GrabDev& G = s.grab;
     d3 d = mk(-G.target[0], -G.target[1], -G.target[2]);
     double wv = 0.0;
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
         d = d + pos(s, G.v[j], v, p) * G.w[j];
         if (G.v[j] == v) wv += G.w[j];
     }
-    double e = 0.5 * G.k * dot(d, d);
     if (D) {
         g = g + d * (G.k * wv);
         sym_add_diag(H, G.k * wv * wv);
     }
-    return e;
+    return 0.5 * G.k * dot(d, d);
 }
 
-// Sum of every incident term (VbdSolver::local, src/vbd.rs:196-248).
-template <bool D>
-__device__ double local_sum(const SweepView& s, uint32_t v, d3 p, d3& g, Sym& H) {
+// Partial sum of the incident terms dealt to `lane` of a group of G
+// (VbdSolver::local, src/vbd.rs:196-248).
+template <bool D, int G>
+__device__ __forceinline__ double local_part(const SweepView& s, uint32_t v, d3 p, uint32_t lane, d3& g, Sym& H) {
     double e = 0.0;
-    for (uint32_t k = s.inc_off[v]; k < s.inc_off[v + 1]; ++k) {
+    uint32_t b1 = s.inc_off[v + 1];
+    for (uint32_t k = s.inc_off[v] + lane; k < b1; k += G) {
         uint32_t ent = s.inc[k];
         uint32_t type = ent >> 30, slot = (ent >> 28) & 3u, idx = ent & 0x0fffffffu;
         if (type == TERM_TRI) e += membrane_term<D>(s, idx, slot, p, g, H);
         else if (type == TERM_HINGE) e += bending_term<D>(s, idx, slot, p, g, H);
         else e += stitch_term<D>(s, idx, v, p, g, H);
     }
-    for (uint32_t k = s.contacts.inc_off[v]; k < s.contacts.inc_off[v + 1]; ++k)
-        e += contact_term<D>(s, s.contacts.inc[k], v, p, g, H);
-    if (s.grab.active && (s.grab.v[0] == v || s.grab.v[1] == v || s.grab.v[2] == v)) e += grab_term<D>(s, v, p, g, H);
+    uint32_t c1 = s.contacts.inc_off[v + 1];
+    for (uint32_t k = s.contacts.inc_off[v] + lane; k < c1; k += G) e += contact_term<D>(s, s.contacts.inc[k], v, p, g, H);
+    if (lane == 0 && s.grab.active && (s.grab.v[0] == v || s.grab.v[1] == v || s.grab.v[2] == v))
+        e += grab_term<D>(s, v, p, g, H);
     return e;
+}
+
+template <int G>
+__device__ __forceinline__ double group_sum(double x, unsigned mask) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) x += __shfl_xor_sync(mask, x, o, G);
+    return x;
 }
 
 __device__ __forceinline__ d3 truncate_ball(const SweepView& s, uint32_t v, d3 proposed, bool& clipped) {  // world.rs:91-100
@@ -448,9 +513,10 @@ __device__ __forceinline__ d3 truncate_ball(const SweepView& s, uint32_t v, d3 p
     return proposed;
 }
 
-__device__ void solve_vertex(const SweepView& s, uint32_t v) {
+template <int G>
+__device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uint32_t lane, unsigned mask) {
     if (s.pinned[v]) {
-        s.residual[v] = 0.0;
+        if (lane == 0) s.residual[v] = 0.0;
         return;
     }
     d3 x = ld3(s.x, v);
@@ -459,7 +525,15 @@ __device__ void solve_vertex(const SweepView& s, uint32_t v) {
     d3 g = mk(0, 0, 0);
     Sym H;
     sym_zero(H);
-    double e_el = local_sum<true>(s, v, x, g, H);
+    double e_el = local_part<true, G>(s, v, x, lane, g, H);
+    if (G > 1) {
+        e_el = group_sum<G>(e_el, mask);
+        g.x = group_sum<G>(g.x, mask);
+        g.y = group_sum<G>(g.y, mask);
+        g.z = group_sum<G>(g.z, mask);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) H.a[k] = group_sum<G>(H.a[k], mask);
+    }
     d3 xy = x - y;
     g = g + xy * m;
     sym_add_diag(H, m);
@@ -487,7 +561,8 @@ __device__ void solve_vertex(const SweepView& s, uint32_t v) {
         truncated = truncated || bound;
         d3 gd;
         Sym Hd;
-        double e = local_sum<false>(s, v, cand, gd, Hd);
+        double e = local_part<false, G>(s, v, cand, lane, gd, Hd);
+        if (G > 1) e = group_sum<G>(e, mask);
         d3 cy = cand - y;
         e += 0.5 * m * dot(cy, cy);
         if (isfin(cand) && isfinite(e) && e <= old + 1e-14) {
@@ -495,21 +570,41 @@ __device__ void solve_vertex(const SweepView& s, uint32_t v) {
             break;
         }
     }
-    st3(s.x, v, accepted);
-    s.residual[v] = dot(g, g);
-    s.clipped_flag[v] = truncated ? 1 : 0;
-    if (truncated) atomicAdd(s.clipped, 1u);
+    if (lane == 0) {
+        st3(s.x, v, accepted);
+        s.residual[v] = dot(g, g);
+        s.clipped_flag[v] = truncated ? 1 : 0;
+        if (truncated) atomicAdd(s.clipped, 1u);
+    }
 }
 
-__global__ void __launch_bounds__(128) k_sweep(SweepView s, const uint32_t* order, uint32_t count) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) solve_vertex(s, order[i]);
+template <int G, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_sweep(SweepView s, const uint32_t* order, uint32_t count) {
+    uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
+    uint32_t gi = t / G;
+    if (gi >= count) return;  // whole groups leave together
+    uint32_t lane = threadIdx.x & (G - 1);
+    unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
+    solve_vertex<G>(s, order[gi], lane, mask);
+}
+
+template <int G>
+static void launch_g(const SweepView& s, const uint32_t* order, uint32_t count, cudaStream_t st) {
+    constexpr int B = 128;
+    uint64_t threads = (uint64_t)count * G;
+    k_sweep<G, B><<<(unsigned)((threads + B - 1) / B), B, 0, st>>>(s, order, count);
 }
 
 void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st) {
-    (void)lanes;
     if (count == 0) return;
-    k_sweep<<<(count + 127) / 128, 128, 0, st>>>(s, order, count);
+    switch (lanes) {
+        case 1: launch_g<1>(s, order, count, st); break;
+        case 2: launch_g<2>(s, order, count, st); break;
+        case 4: launch_g<4>(s, order, count, st); break;
+        case 16: launch_g<16>(s, order, count, st); break;
+        case 32: launch_g<32>(s, order, count, st); break;
+        default: launch_g<8>(s, order, count, st); break;
+    }
 }
 
 // Probe: local e, g, H of every moving vertex at the current positions
@@ -520,7 +615,7 @@ __global__ void k_local_blocks(SweepView s, double* energy, double* grad, double
         d3 g = mk(0, 0, 0);
         Sym H;
         sym_zero(H);
-        double e = local_sum<true>(s, v, x, g, H);
+        double e = local_part<true, 1>(s, v, x, 0, g, H);
         double m = s.inertia ? s.inertia[v] : 0.0;
         d3 y = s.target ? ld3(s.target, v) : x;
         d3 xy = x - y;

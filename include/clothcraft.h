@@ -134,6 +134,8 @@ typedef struct cc_metrics {
     uint64_t vertex_solves;         /* local solves: free vertices x sweeps   */
     uint64_t kernel_launches;       /* launches of this library's kernels     */
     uint64_t contact_incidence;     /* entries of the last contact incidence  */
+    double color_ms;                /* host time spent colouring              */
+    uint64_t color_rounds;          /* greedy-rule rounds of the colourings   */
 } cc_metrics;
 
 /* ContactSet (src/ogc/world.rs:73-107) in caller-owned arrays. The contact
@@ -224,6 +226,12 @@ void* cc_solver_stream(const cc_solver* solver);
 /* When enabled, each colour-sweep launch is bracketed by CUDA events and
  * cc_metrics.sweep_ms reports their summed device time. */
 int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
+/* Threads that cooperate on one vertex's local solve (1, 2, 4, 8, 16 or 32);
+ * 0 (the default) lets the solver time each width on its first step and keep
+ * the fastest. No reference counterpart (the wgpu backend always uses a
+ * 32-lane workgroup per vertex, src/vbd.wgsl:118-150). */
+int32_t cc_solver_set_lanes(cc_solver* solver, int32_t lanes);
+int32_t cc_solver_get_lanes(const cc_solver* solver);
 
 /* The solver's OGC world (owned by the solver; do not destroy). */
 cc_world* cc_solver_world(cc_solver* solver);
