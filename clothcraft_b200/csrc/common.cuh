@@ -28,6 +28,9 @@ inline void cuda_check(cudaError_t e, const char* what) {
 }
 #define CC_CUDA(call) ::cc::cuda_check((call), #call)
 
+// Records the message returned by cc_global_last_error (defined with the C ABI).
+int record_global_error(int code, const std::string& message);
+
 // Device error word bits (set with atomicOr; read by the host once per phase).
 enum DeviceError : uint32_t {
     DERR_NONFINITE_STATE = 1u << 0,

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <set>
 
 #include "world.cuh"
@@ -306,53 +307,64 @@ __device__ bool edge_feasible(const WorldView& w, d3 p, uint32_t e) {  // geomet
     return true;
 }
 
-// closest_triangle (geometry.rs:31-77). kind: 0 vertex, 1 edge, 2 face.
-__device__ d3 closest_triangle(const WorldView& w, d3 p, uint32_t t, int& kind, uint32_t& fid) {
-    uint3 ids = w.tri[t];
-    d3 a = ld3(w.x, ids.x), b = ld3(w.x, ids.y), c = ld3(w.x, ids.z);
+// closest_triangle (geometry.rs:31-77) on explicit corners. kind: 0 vertex,
+// 1 edge, 2 face; which: the corner (0..2) of a vertex feature, or the
+// triangle-edge slot (0 = ab, 1 = bc, 2 = ca) of an edge feature.
+__device__ d3 closest_on_triangle(d3 p, d3 a, d3 b, d3 c, int& kind, int& which) {
     d3 ab = b - a, ac = c - a, ap = p - a;
     double d1 = dot(ab, ap), d2 = dot(ac, ap);
     if (d1 <= 0.0 && d2 <= 0.0) {
         kind = 0;
-        fid = ids.x;
+        which = 0;
         return a;
     }
     d3 bp = p - b;
     double d3_ = dot(ab, bp), d4 = dot(ac, bp);
     if (d3_ >= 0.0 && d4 <= d3_) {
         kind = 0;
-        fid = ids.y;
+        which = 1;
         return b;
     }
     double vc = d1 * d4 - d3_ * d2;
     if (vc <= 0.0 && d1 >= 0.0 && d3_ <= 0.0) {
         kind = 1;
-        fid = w.tri_edges[t].x;
+        which = 0;
         return a + ab * (d1 / (d1 - d3_));
     }
     d3 cp = p - c;
     double d5 = dot(ab, cp), d6 = dot(ac, cp);
     if (d6 >= 0.0 && d5 <= d6) {
         kind = 0;
-        fid = ids.z;
+        which = 2;
         return c;
     }
     double vb = d5 * d2 - d1 * d6;
     if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
         kind = 1;
-        fid = w.tri_edges[t].z;
+        which = 2;
         return a + ac * (d2 / (d2 - d6));
     }
     double va = d3_ * d6 - d5 * d4;
     if (va <= 0.0 && d4 - d3_ >= 0.0 && d5 - d6 >= 0.0) {
         kind = 1;
-        fid = w.tri_edges[t].y;
+        which = 1;
         return b + (c - b) * ((d4 - d3_) / ((d4 - d3_) + (d5 - d6)));
     }
     double denom = 1.0 / (va + vb + vc);
     kind = 2;
-    fid = t;
+    which = 0;
     return a + ab * (vb * denom) + ac * (vc * denom);
+}
+
+// closest_triangle on world triangle t, returning the feature's id.
+__device__ d3 closest_triangle(const WorldView& w, d3 p, uint32_t t, int& kind, uint32_t& fid) {
+    uint3 ids = w.tri[t];
+    int which;
+    d3 q = closest_on_triangle(p, ld3(w.x, ids.x), ld3(w.x, ids.y), ld3(w.x, ids.z), kind, which);
+    if (kind == 0) fid = which == 0 ? ids.x : (which == 1 ? ids.y : ids.z);
+    else if (kind == 1) fid = which == 0 ? w.tri_edges[t].x : (which == 1 ? w.tri_edges[t].y : w.tri_edges[t].z);
+    else fid = t;
+    return q;
 }
 
 __device__ __forceinline__ double clamp01(double x) { return x < 0.0 ? 0.0 : (x > 1.0 ? 1.0 : x); }
@@ -1299,3 +1311,182 @@ void World::download(std::vector<uint32_t>& kind, std::vector<uint32_t>& verts, 
 }
 
 }  // namespace cc
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the narrow-phase distance / radius pass.
+//
+// Some callers cannot call cudaMalloc: an editor's fixed-budget frame worker,
+// where an allocation (and the device-wide synchronisation that cudaFree
+// implies) would stall the frame, and hosts that reserve all device memory
+// up front and hand this library only their own buffers. For them this entry
+// point keeps its per-vertex scratch (the running minimum distance of every
+// vertex) in the file-scope array below instead of allocating it. The caller
+// passes all inputs and outputs as device pointers.
+//
+// The array holds kNoAllocMaxVertices distance slots plus the global minimum
+// and an error word; every GPU that loads the library holds it (2 MiB) until
+// the process exits. Every call shares it and it keeps the previous call's
+// contents, so each call clears what must start from a known value, and two
+// calls whose kernels overlap on the GPU (e.g. on different streams) race.
+namespace cc {
+
+constexpr uint64_t kNoAllocMaxVertices = 262144;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocMaxVertices + 2];
+
+struct NoAllocArgs {
+    const double* x;  // [n_all][3]
+    uint32_t n_all, moving, n_tri, n_edge;
+    const uint32_t* tri;    // [n_tri][3]
+    const uint32_t* edges;  // [n_edge][2]
+    const uint32_t* vf;     // [n_vf][2]: point, triangle
+    const uint32_t* ee;     // [n_ee][2]: edge, edge (reference operand order)
+    unsigned long long n_vf, n_ee;
+    double query_radius, relaxation;
+    unsigned long long* scratch;  // device address of g_noalloc_scratch
+};
+
+__device__ __forceinline__ d3 na_x(const NoAllocArgs& a, uint32_t i) {
+    return mk(a.x[3 * (size_t)i], a.x[3 * (size_t)i + 1], a.x[3 * (size_t)i + 2]);
+}
+
+__global__ void k_noalloc_clear(NoAllocArgs a) {
+    unsigned long long q = dbits(a.query_radius);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_all; i += gridDim.x * blockDim.x)
+        a.scratch[i] = q;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.scratch[kNoAllocMaxVertices] = q;
+        a.scratch[kNoAllocMaxVertices + 1] = 0ull;
+    }
+}
+
+// OgcWorld::scan distances (world.rs:461-524): the minimum over pairs with
+// d < query_radius, for the point and the triangle's corners (VF) and the
+// four edge endpoints (EE). Out-of-range indices set the error word.
+__global__ void k_noalloc_pairs(NoAllocArgs a) {
+    unsigned long long* dist = a.scratch;
+    unsigned long long total = a.n_vf + a.n_ee;
+    for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
+         k += (unsigned long long)gridDim.x * blockDim.x) {
+        if (k < a.n_vf) {
+            uint32_t v = a.vf[2 * k], t = a.vf[2 * k + 1];
+            if (v >= a.n_all || t >= a.n_tri) {
+                atomicOr(&dist[kNoAllocMaxVertices + 1], 1ull);
+                continue;
+            }
+            uint32_t i0 = a.tri[3 * (size_t)t], i1 = a.tri[3 * (size_t)t + 1], i2 = a.tri[3 * (size_t)t + 2];
+            if (i0 >= a.n_all || i1 >= a.n_all || i2 >= a.n_all) {
+                atomicOr(&dist[kNoAllocMaxVertices + 1], 1ull);
+                continue;
+            }
+            d3 xv = na_x(a, v);
+            int kind, which;
+            d3 p = closest_on_triangle(xv, na_x(a, i0), na_x(a, i1), na_x(a, i2), kind, which);
+            double d = len(xv - p);
+            if (d >= a.query_radius) continue;
+            unsigned long long db = dbits(d);
+            atomicMin(&dist[v], db);
+            atomicMin(&dist[i0], db);
+            atomicMin(&dist[i1], db);
+            atomicMin(&dist[i2], db);
+        } else {
+            unsigned long long kk = k - a.n_vf;
+            uint32_t e = a.ee[2 * kk], f = a.ee[2 * kk + 1];
+            if (e >= a.n_edge || f >= a.n_edge) {
+                atomicOr(&dist[kNoAllocMaxVertices + 1], 1ull);
+                continue;
+            }
+            uint32_t e0 = a.edges[2 * (size_t)e], e1 = a.edges[2 * (size_t)e + 1];
+            uint32_t f0 = a.edges[2 * (size_t)f], f1 = a.edges[2 * (size_t)f + 1];
+            if (e0 >= a.n_all || e1 >= a.n_all || f0 >= a.n_all || f1 >= a.n_all) {
+                atomicOr(&dist[kNoAllocMaxVertices + 1], 1ull);
+                continue;
+            }
+            d3 pa = na_x(a, e0), pb = na_x(a, e1), pc = na_x(a, f0), pd = na_x(a, f1);
+            double s, t;
+            closest_segments(pa, pb, pc, pd, s, t);
+            d3 p = pa + (pb - pa) * s;
+            d3 q = pc + (pd - pc) * t;
+            double dist_pq = len(p - q);
+            if (dist_pq >= a.query_radius) continue;
+            unsigned long long db = dbits(dist_pq);
+            atomicMin(&dist[e0], db);
+            atomicMin(&dist[e1], db);
+            atomicMin(&dist[f0], db);
+            atomicMin(&dist[f1], db);
+        }
+    }
+}
+
+// radii = relaxation * d and the minimum over moving vertices (world.rs:394-414)
+__global__ void k_noalloc_radii(NoAllocArgs a, double* radii) {
+    unsigned long long m = dbits(a.query_radius);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.moving; i += gridDim.x * blockDim.x) {
+        unsigned long long b = a.scratch[i];
+        m = min(m, b);
+        radii[i] = a.relaxation * bitsd(b);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMin(&a.scratch[kNoAllocMaxVertices], m);
+}
+
+__global__ void k_noalloc_store_min(NoAllocArgs a, double* minimum_distance) {
+    *minimum_distance = bitsd(a.scratch[kNoAllocMaxVertices]);
+}
+
+}  // namespace cc
+
+namespace {
+std::mutex g_noalloc_mutex;
+unsigned long long* g_noalloc_address[128] = {nullptr};
+}  // namespace
+
+extern "C" int32_t cc_ogc_radii_noalloc(const double* x, uint64_t n_all, uint64_t moving, const uint32_t* triangles,
+                                        uint64_t n_triangles, const uint32_t* edges, uint64_t n_edges,
+                                        const uint32_t* vf_pairs, uint64_t n_vf, const uint32_t* ee_pairs,
+                                        uint64_t n_ee, double query_radius, double relaxation, double* radii,
+                                        double* minimum_distance, void* stream) {
+    using namespace cc;
+    if (n_all > kNoAllocMaxVertices) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf,
+                      "cc_ogc_radii_noalloc: %llu vertices exceed the static scratch limit of %llu vertices",
+                      (unsigned long long)n_all, (unsigned long long)kNoAllocMaxVertices);
+        return record_global_error(CC_ERR_INVALID_ARGUMENT, buf);
+    }
+    if (!x || !radii || !minimum_distance || moving > n_all || (n_vf && (!vf_pairs || !triangles)) ||
+        (n_ee && (!ee_pairs || !edges)) || n_triangles > 0xffffffffull || n_edges > 0xffffffffull ||
+        !std::isfinite(query_radius) || !(query_radius > 0.0) || !std::isfinite(relaxation) ||
+        !(relaxation > 0.0) || !(relaxation < 0.5))
+        return record_global_error(CC_ERR_INVALID_ARGUMENT, "cc_ogc_radii_noalloc: invalid argument");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+        return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: no current CUDA device");
+    unsigned long long* scratch;
+    {
+        // once per device, with that device current: the symbol's device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_address[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
+                return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: scratch address unavailable");
+            g_noalloc_address[dev] = static_cast<unsigned long long*>(p);
+        }
+        scratch = g_noalloc_address[dev];
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    NoAllocArgs a{x, (uint32_t)n_all, (uint32_t)moving, (uint32_t)n_triangles, (uint32_t)n_edges, triangles, edges,
+                  vf_pairs, ee_pairs, n_vf, n_ee, query_radius, relaxation, scratch};
+    k_noalloc_clear<<<grid_for(n_all + 1, 256), 256, 0, st>>>(a);
+    if (n_vf + n_ee) k_noalloc_pairs<<<grid_for((size_t)(n_vf + n_ee), 128), 128, 0, st>>>(a);
+    if (moving) k_noalloc_radii<<<grid_for(moving, 256), 256, 0, st>>>(a, radii);
+    k_noalloc_store_min<<<1, 1, 0, st>>>(a, minimum_distance);
+    if (cudaGetLastError() != cudaSuccess) return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: launch failed");
+    // read the error word back (into a host variable; nothing is allocated)
+    unsigned long long bad = 0;
+    if (cudaMemcpyAsync(&bad, scratch + kNoAllocMaxVertices + 1, sizeof bad, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: device failure");
+    if (bad) return record_global_error(CC_ERR_INVALID_ARGUMENT, "cc_ogc_radii_noalloc: index out of range");
+    return CC_OK;
+}

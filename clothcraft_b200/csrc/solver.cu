@@ -58,6 +58,8 @@ bool vbd_valid(const cc_vbd_settings& s) {  // src/vbd.rs:38-51
 // --------------------------------------------------------------- kernels
 namespace cc {
 
+int record_global_error(int code, const std::string& message) { return set_global(code, message); }
+
 struct StepScalars {
     unsigned int error;
     unsigned int mismatch;

@@ -51,6 +51,9 @@ SIGNATURES = {
                                     C.POINTER(cc_contacts)]),
     "cc_world_candidates": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_candidates)]),
     "cc_world_edges": (C.c_uint64, [C.c_void_p, c_uint32_p]),
+    "cc_ogc_radii_noalloc": (C.c_int32, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
+                                         C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_double,
+                                         C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 

@@ -272,6 +272,35 @@ int32_t cc_world_candidates(cc_world* world, const double* x, double radius,
 /* Topology sizes: edges of the combined mesh (src/ogc/topology.rs:13-52). */
 uint64_t cc_world_edges(const cc_world* world, uint32_t* edges_out);
 
+/* ------------------------------------------------------- allocation-free */
+/* No counterpart in the reference. Per-vertex OGC distances and conservative
+ * radii for given candidate pairs, without allocating any memory, for callers
+ * that cannot call cudaMalloc: a fixed-budget frame worker for which an
+ * allocation (and the device-wide synchronisation cudaFree implies) would
+ * stall the frame, or a host that reserves all device memory at start-up and
+ * passes this library only its own buffers.
+ *
+ * ALL pointers are device pointers: x [n_all][3]; triangles [n_triangles][3];
+ * edges [n_edges][2] (as cc_world_edges returns them); vf_pairs [n_vf][2]
+ * (point, triangle) and ee_pairs [n_ee][2] (edge, edge), e.g. the lists of
+ * cc_world_candidates at a search radius >= query_radius; outputs radii
+ * [moving] and *minimum_distance. Results equal the radii and minimum
+ * distance of cc_world_detect for the same positions and query radius.
+ *
+ * The per-vertex scratch is a static device array of 262,144 vertex slots
+ * (2 MiB, held by every GPU that loads the library until exit); larger
+ * n_all is rejected with CC_ERR_INVALID_ARGUMENT and a message. Kernels run
+ * on `stream` (a cudaStream_t; NULL = legacy default stream) and the call
+ * returns after they finish. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture. All calls share the one
+ * array, so calls whose kernels overlap on the GPU race. */
+int32_t cc_ogc_radii_noalloc(const double* x, uint64_t n_all, uint64_t moving, const uint32_t* triangles,
+                             uint64_t n_triangles, const uint32_t* edges, uint64_t n_edges,
+                             const uint32_t* vf_pairs, uint64_t n_vf, const uint32_t* ee_pairs, uint64_t n_ee,
+                             double query_radius, double relaxation, double* radii, double* minimum_distance,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif
