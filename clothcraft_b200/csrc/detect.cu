@@ -999,8 +999,10 @@ void World::build_candidates(double R, double skin) {
     LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
     LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
     if (vf_cap_ == 0) {
-        vf_cap_ = std::max<size_t>(1024, 16 * n_all_);
-        ee_cap_ = std::max<size_t>(1024, 32 * n_edge_);
+        // generous first capacities: the in-plane pairs of a sheet at the
+        // candidate radius alone reach ~60 per edge
+        vf_cap_ = std::max<size_t>(1024, 48 * n_all_);
+        ee_cap_ = std::max<size_t>(1024, 96 * n_edge_);
     }
     for (int attempt = 0; attempt < 8; ++attempt) {
         vf_.reserve(vf_cap_);
@@ -1018,12 +1020,12 @@ void World::build_candidates(double R, double skin) {
         raise_device_error(stats_h_.ptr->error);
         bool grow = false;
         if (stats_h_.ptr->n_vf > vf_cap_) {
-            vf_cap_ = (size_t)(stats_h_.ptr->n_vf * 1.25) + 1024;
+            vf_cap_ = (size_t)(stats_h_.ptr->n_vf * 1.5) + 1024;
             vf_.release();
             grow = true;
         }
         if (stats_h_.ptr->n_ee > ee_cap_) {
-            ee_cap_ = (size_t)(stats_h_.ptr->n_ee * 1.25) + 1024;
+            ee_cap_ = (size_t)(stats_h_.ptr->n_ee * 1.5) + 1024;
             ee_.release();
             grow = true;
         }
@@ -1079,7 +1081,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
     }
     unsigned long long n_vf = stats_h_.ptr->n_vf, n_ee = stats_h_.ptr->n_ee;
     // narrow phase
-    if (raw_cap_ == 0) raw_cap_ = std::max<size_t>(4096, (size_t)(n_vf + n_ee) / 4 + 4096);
+    if (raw_cap_ == 0) raw_cap_ = std::max<size_t>(4096, (size_t)(n_vf + n_ee) / 2 + 4096);
     for (int attempt = 0; attempt < 8; ++attempt) {
         raw_hi_.reserve(raw_cap_);
         raw_lo_.reserve(raw_cap_);
@@ -1099,7 +1101,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
         CC_CUDA(cudaGetLastError());
         sync_stats();
         if (stats_h_.ptr->n_raw <= raw_cap_) break;
-        raw_cap_ = (size_t)(stats_h_.ptr->n_raw * 1.25) + 4096;
+        raw_cap_ = (size_t)(stats_h_.ptr->n_raw * 1.5) + 4096;
         raw_hi_.release();
         raw_lo_.release();
         raw_eps_.release();
@@ -1121,7 +1123,6 @@ void World::detect(double query_radius, double radius, double relaxation, double
         cub::DeviceScan::ExclusiveSum(nullptr, need2, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw, stream_);
         need = std::max(need, need2);
         if (need > cub_tmp_bytes_) {
-            cub_tmp_.release();
             cub_tmp_.reserve(need);
             cub_tmp_bytes_ = need;
         }
@@ -1160,7 +1161,6 @@ void World::detect(double query_radius, double radius, double relaxation, double
         size_t need = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1), stream_);
         if (need > cub_tmp_bytes_) {
-            cub_tmp_.release();
             cub_tmp_.reserve(need);
             cub_tmp_bytes_ = need;
         }
@@ -1182,8 +1182,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
             size_t need = 0;
             cub::DeviceRadixSort::SortKeys(nullptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0, 64, stream_);
             if (need > cub_tmp_bytes_) {
-                cub_tmp_.release();
-                cub_tmp_.reserve(need);
+                    cub_tmp_.reserve(need);
                 cub_tmp_bytes_ = need;
             }
             CC_CUDA(cub::DeviceRadixSort::SortKeys(cub_tmp_.ptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0,

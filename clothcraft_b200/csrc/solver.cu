@@ -64,7 +64,8 @@ struct StepScalars {
     unsigned int error;
     unsigned int mismatch;
     unsigned int clipped;
-    unsigned int pad;
+    unsigned int refresh_at;  // first iteration whose start needs a refresh detection
+    unsigned int clipped_iter[256];
     unsigned long long motion_bits;
     unsigned long long seam_gap_bits;
     double residual;
@@ -139,6 +140,15 @@ __global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* g
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&sc->clipped, cnt);
+}
+
+// Refresh rule after iteration `it` (src/vbd.rs:326): the next iteration
+// starts with a new detection when at least refresh_fraction * n vertices
+// were clipped. Later sweeps already enqueued see refresh_at and skip.
+__global__ void k_refresh_rule(StepScalars* sc, uint32_t it, uint32_t iterations, double threshold) {
+    if (sc->refresh_at <= it) return;  // this iteration was skipped
+    unsigned int c = sc->clipped_iter[it];
+    if (c > 0 && (double)c >= threshold && it + 1 < iterations) sc->refresh_at = it + 1;
 }
 
 // finite result and trust-region invariant (src/vbd.rs:399-405), residual sum
@@ -261,7 +271,7 @@ struct cc_solver {
     DBuf<double> ext_w, ext_w_s, ext_cum;
     DBuf<unsigned char> cub_tmp;
     size_t cub_bytes = 0;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, tune0 = nullptr, tune1 = nullptr;
     bool profiling = false;
     std::vector<cudaEvent_t> prof_events;
     uint64_t own_launches = 0;
@@ -280,6 +290,8 @@ struct cc_solver {
         world.reset();
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (tune0) cudaEventDestroy(tune0);
+        if (tune1) cudaEventDestroy(tune1);
         for (auto e : prof_events) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -361,8 +373,11 @@ struct cc_solver {
 
 // Project autotuner: time one full colour sweep per candidate group width on
 // a backup of the positions (restored after each trial) and keep the fastest.
-void cc_solver::autotune(const SweepView& sv) {
+void cc_solver::autotune(const SweepView& sv_in) {
     static const int kCandidates[] = {1, 2, 4, 8, 16, 32};
+    SweepView sv = sv_in;  // trial sweeps never skip and count into a scratch counter
+    sv.skip_at = nullptr;
+    sv.clipped = &sc.ptr->clipped;
     x_backup.reserve(n);
     CC_CUDA(cudaMemcpyAsync(x_backup.ptr, world->x(), n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
     const auto& off = coloring.offsets();
@@ -372,17 +387,18 @@ void cc_solver::autotune(const SweepView& sv) {
     for (int g : kCandidates) {
         float total = 1e30f;
         for (int rep = 0; rep < 4; ++rep) {  // first repetition warms caches; keep the fastest of the rest
-            CC_CUDA(cudaEventRecord(ev0, stream));
-            for (uint32_t c = 0; c < coloring.n_colors(); ++c)
-                launch_sweep(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
-            CC_CUDA(cudaEventRecord(ev1, stream));
+            CC_CUDA(cudaEventRecord(tune0, stream));
+            for (int sweep = 0; sweep < 2; ++sweep)  // two consecutive sweeps, as the iterations run
+                for (uint32_t c = 0; c < coloring.n_colors(); ++c)
+                    launch_sweep(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
+            CC_CUDA(cudaEventRecord(tune1, stream));
             CC_CUDA(cudaMemcpyAsync(world->x(), x_backup.ptr, n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
-            CC_CUDA(cudaEventSynchronize(ev1));
+            CC_CUDA(cudaEventSynchronize(tune1));
             CC_CUDA(cudaGetLastError());
             float t = 0.f;
-            CC_CUDA(cudaEventElapsedTime(&t, ev0, ev1));
+            CC_CUDA(cudaEventElapsedTime(&t, tune0, tune1));
             if (rep > 0) total = std::min(total, t);
-            own_launches += coloring.n_colors();
+            own_launches += 2 * coloring.n_colors();
         }
         tune_ms.push_back(total);
         if (total < best) {
@@ -448,41 +464,68 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     CC_CUDA(cudaGetLastError());
     read_scalars();
     size_t clipped = sc_h.ptr->clipped;
-    for (uint32_t it = 0; it < s.iterations; ++it) {
-        if (clipped > 0 && (double)clipped >= s.contact.refresh_fraction * (double)n) {
+    // Every remaining iteration is enqueued at once; k_refresh_rule decides
+    // each refresh on the device and the host syncs once per batch, redoing
+    // from the first iteration that needed a refresh (sweeps enqueued past it
+    // exit immediately).
+    const double threshold = s.contact.refresh_fraction * (double)n;
+    bool need_refresh = clipped > 0 && (double)clipped >= threshold;
+    std::vector<std::pair<size_t, uint32_t>> prof_pairs;  // (event index, iteration)
+    std::vector<uint32_t> prof_ok;
+    uint32_t it0 = 0;
+    while (it0 < s.iterations) {
+        if (need_refresh) {
             detect(rq, s.contact, &m, det_ms);
             cv = world->contacts();
             color(cv, grab, m);
         }
         SweepView sv = sweep_view(cv, s, grab);
+        sv.skip_at = &sc.ptr->refresh_at;
         if (lanes == 0) autotune(sv);
-        CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->refresh_at, 0xff, sizeof(unsigned int), stream));
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_iter[it0], 0, (s.iterations - it0) * sizeof(unsigned int), stream));
         const auto& off = coloring.offsets();
-        for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
-            uint32_t cnt = off[c + 1] - off[c];
-            if (cnt == 0) continue;
-            if (profiling) {
-                while (prof_events.size() < prof_used + 2) {
-                    cudaEvent_t e;
-                    CC_CUDA(cudaEventCreate(&e));
-                    prof_events.push_back(e);
+        size_t batch_first_pair = prof_pairs.size();
+        for (uint32_t it = it0; it < s.iterations; ++it) {
+            sv.iteration = it;
+            sv.clipped = &sc.ptr->clipped_iter[it];
+            for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
+                uint32_t cnt = off[c + 1] - off[c];
+                if (cnt == 0) continue;
+                if (profiling) {
+                    while (prof_events.size() < prof_used + 2) {
+                        cudaEvent_t e;
+                        CC_CUDA(cudaEventCreate(&e));
+                        prof_events.push_back(e);
+                    }
+                    CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
                 }
-                CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
+                launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
+                if (profiling) {
+                    CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
+                    prof_pairs.push_back({prof_used, it});
+                    prof_used += 2;
+                }
+                ++own_launches;
             }
-            launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
-            if (profiling) {
-                CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
-                prof_used += 2;
-            }
+            k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold);
             ++own_launches;
-            ++m.sweep_launches;
         }
-        m.vertex_solves += n_free;
         CC_CUDA(cudaGetLastError());
         read_scalars();
-        clipped = sc_h.ptr->clipped;
-        m.truncated_vertices += clipped;
+        uint32_t ra = sc_h.ptr->refresh_at;
+        uint32_t done_to = ra < s.iterations ? ra : s.iterations;
+        m.sweep_launches += (uint64_t)(done_to - it0) * coloring.n_colors();
+        for (size_t k = batch_first_pair; k < prof_pairs.size(); ++k) prof_ok.push_back(prof_pairs[k].second < done_to);
+        if (ra < s.iterations) {
+            it0 = ra;
+            need_refresh = true;
+        } else {
+            it0 = s.iterations;
+        }
     }
+    for (uint32_t it = 0; it < s.iterations; ++it) m.truncated_vertices += sc_h.ptr->clipped_iter[it];
+    m.vertex_solves = (uint64_t)n_free * s.iterations;
     m.colors = coloring.n_colors();
     CC_CUDA(cudaMemsetAsync(&sc.ptr->residual, 0, sizeof(double), stream));
     k_step_finish<<<gb, 256, 0, stream>>>(n, world->x(), cv, residual.ptr, sc.ptr);
@@ -516,7 +559,6 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         cub::DeviceScan::InclusiveSum(nullptr, need2, ext_w_s.ptr, ext_cum.ptr, (int)n_tri, stream);
         need = std::max(need, need2);
         if (need > cub_bytes) {
-            cub_tmp.release();
             cub_tmp.reserve(need);
             cub_bytes = need;
         }
@@ -556,9 +598,10 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     m.gpu_compute_ms = gms;
     if (profiling) {
         double sw = 0.0;
-        for (size_t k = 0; k < prof_used; k += 2) {
+        for (size_t k = 0; k < prof_pairs.size(); ++k) {
+            if (!prof_ok[k]) continue;  // enqueued past a refresh and skipped
             float t = 0.f;
-            CC_CUDA(cudaEventElapsedTime(&t, prof_events[k], prof_events[k + 1]));
+            CC_CUDA(cudaEventElapsedTime(&t, prof_events[prof_pairs[k].first], prof_events[prof_pairs[k].first + 1]));
             sw += t;
         }
         m.sweep_ms = sw;
@@ -609,6 +652,8 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         CC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         CC_CUDA(cudaEventCreate(&h->ev0));
         CC_CUDA(cudaEventCreate(&h->ev1));
+        CC_CUDA(cudaEventCreate(&h->tune0));
+        CC_CUDA(cudaEventCreate(&h->tune1));
         cudaStream_t st = h->stream;
         h->n = (uint32_t)n;
         // pins must match their constraints (src/vbd.rs:110-120)

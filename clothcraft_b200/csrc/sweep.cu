@@ -580,6 +580,7 @@ __device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uin
 
 template <int G, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_sweep(SweepView s, const uint32_t* order, uint32_t count) {
+    if (s.skip_at && *s.skip_at <= s.iteration) return;  // a refresh detection precedes this iteration
     uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
     uint32_t gi = t / G;
     if (gi >= count) return;  // whole groups leave together

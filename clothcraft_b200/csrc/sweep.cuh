@@ -45,6 +45,8 @@ struct SweepView {
     GrabDev grab;
     double* residual;           // [n] |g|^2 of the vertex's last solve
     unsigned int* clipped;      // counter
+    const unsigned int* skip_at;  // sweeps of iterations >= *skip_at exit at once (null: never)
+    uint32_t iteration;
     unsigned char* clipped_flag;  // [n]
 };
 

@@ -92,6 +92,11 @@ def lib():
             "or_greedy_colors": (C.c_uint32, [C.c_uint64, c_uint64_p, c_uint32_p, C.POINTER(cc_contacts),
                                               C.POINTER(cc_grab), c_uint32_p]),
             "or_extension_percent": (None, [C.POINTER(cc_mesh), c_double_p, c_double_p]),
+            "or_newton_step": (C.c_int32, [vp, c_double_p, c_double_p, C.POINTER(cc_vbd_settings), C.c_int32,
+                                           C.c_int32, C.c_double, C.c_double, C.c_int32, c_double_p, c_double_p,
+                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "or_step_gradient": (C.c_int32, [vp, c_double_p, c_double_p, C.POINTER(cc_vbd_settings), c_double_p,
+                                             C.c_int32, c_double_p, c_double_p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -262,6 +267,48 @@ class Solver:
         if rc != 0:
             raise self._err(rc)
         return x, v, t.value, m.as_dict()
+
+    def newton_step(self, x_old, v_old, settings: cc_vbd_settings, newton_iterations=30, pcg_iterations=250,
+                    abs_tol=1e-6, rel_tol=1e-4, threads=8):
+        """FP64 Newton-PCG step (src/solver.rs:422-646) with the OGC contacts
+        detected at x_old frozen. Returns (x, residual_rms, converged, iterations)."""
+        xo = abi.as_f64(x_old)
+        vo = abi.as_f64(v_old)
+        out = np.zeros((self.n, 3))
+        res = C.c_double()
+        conv = C.c_int32()
+        its = C.c_int32()
+        rc = lib().or_newton_step(self.h, f64p(xo), f64p(vo), C.byref(settings), newton_iterations, pcg_iterations,
+                                  abs_tol, rel_tol, threads, f64p(out), C.byref(res), C.byref(conv), C.byref(its))
+        if rc != 0:
+            raise OracleError(rc, "Newton step failed")
+        return out, res.value, bool(conv.value), its.value
+
+    def step_gradient(self, x_old, v_old, settings: cc_vbd_settings, x_eval, threads=8):
+        """Objective and gradient (pinned dofs zero) of the step from
+        (x_old, v_old) at x_eval, OGC contacts detected at x_old frozen."""
+        xo = abi.as_f64(x_old)
+        vo = abi.as_f64(v_old)
+        xe = abi.as_f64(x_eval)
+        g = np.zeros((self.n, 3))
+        e = C.c_double()
+        rc = lib().or_step_gradient(self.h, f64p(xo), f64p(vo), C.byref(settings), f64p(xe), threads, C.byref(e),
+                                    f64p(g))
+        if rc != 0:
+            raise OracleError(rc, "objective evaluation failed")
+        return e.value, g
+
+    def relative_residual(self, x_old, v_old, settings: cc_vbd_settings, x_eval, threads=8):
+        """||grad E(x_eval)|| / ||grad E(y)|| over free vertices, y the
+        inertial target (the step's convergence measure)."""
+        xo = abi.as_f64(x_old).reshape(-1, 3)
+        vo = abi.as_f64(v_old).reshape(-1, 3)
+        damp = 1.0 + settings.damping * settings.dt
+        g = np.array([settings.gravity[0], settings.gravity[1], settings.gravity[2]])
+        y = xo + (vo * settings.dt + g * settings.dt * settings.dt) / damp
+        _, gx = self.step_gradient(xo, vo, settings, x_eval, threads)
+        _, gy = self.step_gradient(xo, vo, settings, y, threads)
+        return float(np.linalg.norm(gx) / np.linalg.norm(gy))
 
     def colors(self, x_all, query_radius, ogc: cc_ogc_settings, grab=None):
         x_all = abi.as_f64(x_all)

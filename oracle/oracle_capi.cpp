@@ -624,3 +624,5 @@ void or_extension_percent(const cc_mesh* mesh, const double* x, double* out2) {
 }
 
 }  // extern "C"
+
+extern "C" VbdSolver* or_solver_inner(or_solver* s) { return &s->s; }
