@@ -374,7 +374,9 @@ struct cc_solver {
 // Project autotuner: time one full colour sweep per candidate group width on
 // a backup of the positions (restored after each trial) and keep the fastest.
 void cc_solver::autotune(const SweepView& sv_in) {
-    static const int kCandidates[] = {1, 2, 4, 8, 16, 32};
+    // lanes per vertex | register cap (3 or 4 resident 128-thread blocks per SM) << 8
+    static const int kCandidates[] = {1 | 3 << 8, 2 | 3 << 8,  4 | 3 << 8,  4 | 4 << 8, 8 | 3 << 8,
+                                      8 | 4 << 8, 16 | 3 << 8, 16 | 4 << 8, 32 | 3 << 8};
     SweepView sv = sv_in;  // trial sweeps never skip and count into a scratch counter
     sv.skip_at = nullptr;
     sv.clipped = &sc.ptr->clipped;
@@ -383,7 +385,7 @@ void cc_solver::autotune(const SweepView& sv_in) {
     const auto& off = coloring.offsets();
     tune_ms.clear();
     float best = 1e30f;
-    int best_g = 8;
+    int best_g = 8 | 3 << 8;
     for (int g : kCandidates) {
         float total = 1e30f;
         for (int rep = 0; rep < 4; ++rep) {  // first repetition warms caches; keep the fastest of the rest
@@ -863,10 +865,10 @@ int32_t cc_solver_set_profiling(cc_solver* s, int32_t enable) {
 int32_t cc_solver_set_lanes(cc_solver* s, int32_t lanes) {
     if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32))
         return s->fail(Failure{CC_ERR_INVALID_ARGUMENT, "lanes must be 0 (autotune) or a power of two up to 32"});
-    s->lanes = lanes;
+    s->lanes = lanes == 0 ? 0 : (lanes | 3 << 8);
     return CC_OK;
 }
-int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes; }
+int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes & 0xff; }
 cc_world* cc_solver_world(cc_solver* s) { return &s->world_view; }
 
 static void upload_state(cc_solver* s, const double* x, const double* v) {

@@ -57,10 +57,11 @@ __device__ __forceinline__ void sym_add_diag(Sym& h, double s) {
 // axial (src/energy.rs:10-16) with its first and second derivative.
 __device__ __forceinline__ void axial3(double s, double k, double c, double delta, double& f, double& f1, double& f2) {
     double r = sqrt(s * s + delta * delta);
+    double ir = 1.0 / r;
     double p = (s + r - delta) * 0.5;
     f = 0.5 * k * (c * s * s + (1.0 - c) * p * p);
-    double p1 = 0.5 * (1.0 + s / r);
-    double p2 = 0.5 * delta * delta / (r * r * r);
+    double p1 = 0.5 * (1.0 + s * ir);
+    double p2 = 0.5 * delta * delta * (ir * ir * ir);
     f1 = k * (c * s + (1.0 - c) * p * p1);
     f2 = k * (c + (1.0 - c) * (p1 * p1 + p * p2));
 }
@@ -139,15 +140,14 @@ __device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, 
     d3 e = x1 - x0, u = x2 - x0, w = x3 - x0;
     d3 n1 = cross(e, u);
     d3 n2 = cross(w, e);
-    double l1 = sqrt(dot(n1, n1));
-    double l2 = sqrt(dot(n2, n2));
-    d3 h1 = n1 / l1, h2 = n2 / l2;
+    double il1 = rsqrt(dot(n1, n1));
+    double il2 = rsqrt(dot(n2, n2));
+    d3 h1 = n1 * il1, h2 = n2 * il2;
     d3 d = h1 - h2;
     double energy = K * dot(d, d);
     if (!D) return energy;
     d3 a1 = slot == 0 ? u - e : (slot == 1 ? -u : (slot == 2 ? e : mk(0, 0, 0)));
     d3 a2 = slot == 0 ? e - w : (slot == 1 ? w : (slot == 3 ? -e : mk(0, 0, 0)));
-    double il1 = 1.0 / l1, il2 = 1.0 / l2;
     // gradient 2K J^T d with J^T d = sum_k s_k ((P_k d) x a_k) / l_k
     d3 pd1 = d - h1 * dot(h1, d), pd2 = d - h2 * dot(h2, d);
     d3 jtd = cross(pd1, a1) * il1 - cross(pd2, a2) * il2;
@@ -578,8 +578,9 @@ __device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uin
     }
 }
 
-template <int G, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_sweep(SweepView s, const uint32_t* order, uint32_t count) {
+// MINB blocks of BLOCK threads per SM caps the registers (65536 / (MINB*BLOCK)).
+template <int G, int BLOCK, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_sweep(SweepView s, const uint32_t* order, uint32_t count) {
     if (s.skip_at && *s.skip_at <= s.iteration) return;  // a refresh detection precedes this iteration
     uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
     uint32_t gi = t / G;
@@ -590,21 +591,25 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(SweepView s, const uint32_t* or
 }
 
 template <int G>
-static void launch_g(const SweepView& s, const uint32_t* order, uint32_t count, cudaStream_t st) {
+static void launch_g(const SweepView& s, const uint32_t* order, uint32_t count, int minb, cudaStream_t st) {
     constexpr int B = 128;
     uint64_t threads = (uint64_t)count * G;
-    k_sweep<G, B><<<(unsigned)((threads + B - 1) / B), B, 0, st>>>(s, order, count);
+    unsigned grid = (unsigned)((threads + B - 1) / B);
+    if (minb >= 4) k_sweep<G, B, 4><<<grid, B, 0, st>>>(s, order, count);
+    else k_sweep<G, B, 3><<<grid, B, 0, st>>>(s, order, count);
 }
 
-void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st) {
+// variant = lanes per vertex (1..32) | occupancy cap (blocks per SM) << 8
+void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st) {
     if (count == 0) return;
+    int lanes = variant & 0xff, minb = variant >> 8;
     switch (lanes) {
-        case 1: launch_g<1>(s, order, count, st); break;
-        case 2: launch_g<2>(s, order, count, st); break;
-        case 4: launch_g<4>(s, order, count, st); break;
-        case 16: launch_g<16>(s, order, count, st); break;
-        case 32: launch_g<32>(s, order, count, st); break;
-        default: launch_g<8>(s, order, count, st); break;
+        case 1: launch_g<1>(s, order, count, minb, st); break;
+        case 2: launch_g<2>(s, order, count, minb, st); break;
+        case 4: launch_g<4>(s, order, count, minb, st); break;
+        case 16: launch_g<16>(s, order, count, minb, st); break;
+        case 32: launch_g<32>(s, order, count, minb, st); break;
+        default: launch_g<8>(s, order, count, minb, st); break;
     }
 }
 
