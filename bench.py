@@ -48,6 +48,18 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def sweep_traffic():
+    """DRAM bytes per k_sweep launch recorded from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_sweep_sheet256_fold.md")) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def workload():
     from clothcraft_b200 import scenes
 
@@ -222,6 +234,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lanes", type=int, default=0,
+                    help="lanes per vertex solve (1..32); 0 = autotune on the first step")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -253,6 +267,9 @@ def main():
     sc = workload()
     st = sc.settings.to_c()
     solver = VbdSolver(sc)
+    if args.lanes:
+        if L.cc_solver_set_lanes(solver.h, args.lanes) != 0:
+            raise SystemExit("invalid --lanes %d" % args.lanes)
     stream = torch.cuda.ExternalStream(L.cc_solver_stream(solver.h))
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     solver.set_state(*fold_state())
@@ -276,17 +293,15 @@ def main():
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs), metrics
 
-    # ---- device-resident throughput (value)
-    L.cc_solver_set_profiling(solver.h, 1)
+    # ---- device-resident throughput (value); clocks sampled over all GPU legs
+    clocks = ClockSampler(local).__enter__()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        ms, mets = timed(lambda: solver.step_resident(st), args.steps)
+    ms, mets = timed(lambda: solver.step_resident(st), args.steps)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    L.cc_solver_set_profiling(solver.h, 0)
     t_max = ms
     if dist:
         tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -313,6 +328,14 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_max = float(tt.item())
     e2e_value = world * args.steps / (e2e_max / 1000.0)
+
+    # ---- per-launch sweep timing (events around every sweep launch), same
+    # state and step count as the value leg, for the roofline
+    solver.set_state(*warm_state)
+    L.cc_solver_set_profiling(solver.h, 1)
+    _, mets = timed(lambda: solver.step_resident(st), args.steps)
+    L.cc_solver_set_profiling(solver.h, 0)
+    clocks.__exit__(None, None, None)
 
     # ---- roofline of the dominant kernel (colour sweep)
     peak, peak_kind = load_peaks()
@@ -361,11 +384,14 @@ def main():
             "peak": peak,
             "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None,
-            "traffic": None,
+            "traffic": sweep_traffic(),
+            "traffic_note": "dram read+write bytes per k_sweep launch from one ncu capture "
+                            "(profiles/k_sweep_sheet256_fold.md, cold cache)",
             "peak_kind": peak_kind,
             "sweep_launches": int(sweeps),
             "avg_launch_us": 1000.0 * sweep_ms / max(sweeps, 1),
             "algorithmic_bytes_per_step": alg_bytes / args.steps,
+            "algorithmic_bytes_per_launch": alg_bytes / max(sweeps, 1),
             "sweep_share_of_step": sweep_ms / ms if ms > 0 else None,
         },
         "cpu_baseline": cpu,

@@ -76,10 +76,13 @@ class cc_vbd_settings(C.Structure):
     _fields_ = [
         ("dt", C.c_double),
         ("iterations", C.c_uint32),
-        ("reserved0", C.c_uint32),
+        ("init_mode", C.c_uint32),
         ("damping", C.c_double),
         ("gravity", C.c_double * 3),
         ("contact", cc_ogc_settings),
+        ("residual_tolerance", C.c_double),
+        ("residual_check_every", C.c_uint32),
+        ("reserved0", C.c_uint32),
     ]
 
 
@@ -105,11 +108,17 @@ class cc_metrics(C.Structure):
         ("has_residual", C.c_int32), ("reserved0", C.c_int32),
         ("sweep_ms", C.c_double)] + [(n, C.c_uint64) for n in (
             "sweep_launches", "vertex_solves", "kernel_launches", "contact_incidence")] + [
-        ("color_ms", C.c_double), ("color_rounds", C.c_uint64)]
+        ("color_ms", C.c_double), ("color_rounds", C.c_uint64),
+        ("relative_residual", C.c_double), ("initial_relative_residual", C.c_double),
+        ("has_relative_residual", C.c_int32), ("init_used", C.c_int32),
+        ("init_energy_adaptive", C.c_double), ("init_energy_learned", C.c_double),
+        ("init_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
         d["residual_rms_n"] = d["residual_rms_n"] if d.pop("has_residual") else None
+        if not d.pop("has_relative_residual"):
+            d["relative_residual"] = d["initial_relative_residual"] = None
         return d
 
 

@@ -21,6 +21,8 @@ UNITS = {
     "detect.cu": ["--fmad=false"],
     "sweep.cu": [],
     "color.cu": [],
+    "learned.cu": [],
+    "mlp_tc.cu": [],
     "solver.cu": [],
 }
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -15,6 +15,7 @@
 #include <set>
 
 #include "color.cuh"
+#include "learned.cuh"
 #include "sweep.cuh"
 #include "world.cuh"
 
@@ -64,12 +65,21 @@ struct StepScalars {
     unsigned int error;
     unsigned int mismatch;
     unsigned int clipped;
-    unsigned int refresh_at;  // first iteration whose start needs a refresh detection
+    unsigned int refresh_at;    // first iteration whose start needs a refresh detection
+    unsigned int converged_at;  // iterations run when the residual target was met
+    unsigned int stop_at;       // min(refresh_at, converged_at): later sweeps exit at once
+    unsigned int checked_at;    // iterations run at the last residual evaluation
+    unsigned int clipped_alt;   // clipped vertices of the learned guess
     unsigned int clipped_iter[256];
     unsigned long long motion_bits;
     unsigned long long seam_gap_bits;
     double residual;
     double ext_total;
+    double gy2;        // |grad E(y)|^2, y the inertial target
+    double gx2;        // |grad E(x)|^2 at the last evaluation
+    double gx2_init;   // |grad E|^2 of the initial guess
+    double e_init[2];  // step energy of the adaptive / learned initial guess
+    int init_used;
 };
 
 __global__ void k_step_begin(uint32_t n, const double4* x0, const double4* v0, const double4* px, const double4* pv,
@@ -123,7 +133,7 @@ __global__ void k_copy_positions(uint32_t n, const double4* src, double4* dst) {
 
 // Conservative warm start (src/vbd.rs:316-324)
 __global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* guess, ContactsView c, double4* x,
-                             StepScalars* sc) {
+                             unsigned int* clipped) {
     unsigned int cnt = 0;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (pinned[i]) continue;
@@ -139,16 +149,55 @@ __global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* g
         st3(x, i, p);
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&sc->clipped, cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(clipped, cnt);
 }
 
 // Refresh rule after iteration `it` (src/vbd.rs:326): the next iteration
 // starts with a new detection when at least refresh_fraction * n vertices
 // were clipped. Later sweeps already enqueued see refresh_at and skip.
 __global__ void k_refresh_rule(StepScalars* sc, uint32_t it, uint32_t iterations, double threshold) {
-    if (sc->refresh_at <= it) return;  // this iteration was skipped
+    if (sc->stop_at <= it) return;  // this iteration was skipped
     unsigned int c = sc->clipped_iter[it];
-    if (c > 0 && (double)c >= threshold && it + 1 < iterations) sc->refresh_at = it + 1;
+    if (c > 0 && (double)c >= threshold && it + 1 < iterations) {
+        sc->refresh_at = it + 1;
+        sc->stop_at = min(sc->stop_at, it + 1);
+    }
+}
+
+// Relative-residual rule after iteration `it`: |grad E(x)|^2 from the
+// partial sums; with a target, iterations stop at the first evaluation with
+// |grad E(x)| <= tol |grad E(y)|. No reference counterpart (the reference
+// always runs `iterations` sweeps).
+__global__ void __launch_bounds__(256) k_residual_rule(StepScalars* sc, const double* partial, uint32_t it,
+                                                       uint32_t iterations, double tol2, int stop) {
+    if (sc->stop_at <= it) return;  // uniform: every thread reads it before thread 0 writes
+    double g2 = block_sum_partials(partial);
+    if (threadIdx.x == 0) {
+        sc->gx2 = g2;
+        sc->checked_at = it + 1;
+        if (stop && g2 <= tol2 * sc->gy2 && sc->converged_at > it + 1) {
+            sc->converged_at = it + 1;
+            if (it + 1 < iterations) sc->stop_at = min(sc->stop_at, it + 1);
+        }
+    }
+}
+
+// Sum of the partials into *out (one block of 256 threads).
+__global__ void __launch_bounds__(256) k_store_sum(const double* partial, double* out) {
+    double v = block_sum_partials(partial);
+    if (threadIdx.x == 0) *out = v;
+}
+
+// Keep the learned guess (already in `alt`, moving part) when its step
+// energy is not higher than the adaptive guess's (in `x`).
+__global__ void k_select_guess(uint32_t n, const double4* alt, double4* x, StepScalars* sc) {
+    bool learned = sc->e_init[1] <= sc->e_init[0];
+    if (!learned) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = alt[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        sc->clipped = sc->clipped_alt;
+        sc->init_used = 1;
+    }
 }
 
 // finite result and trust-region invariant (src/vbd.rs:399-405), residual sum
@@ -237,6 +286,24 @@ struct cc_world {
     }
 };
 
+struct cc_mlp {
+    std::unique_ptr<Mlp> net;
+    cudaStream_t stream = nullptr;
+    DBuf<uint32_t> perm;
+    DBuf<float> losses;
+    std::string err;
+    int code = 0;
+    int fail(const Failure& f) {
+        err = f.message;
+        code = f.code;
+        return f.code;
+    }
+    ~cc_mlp() {
+        net.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
 struct cc_solver {
     cudaStream_t stream = nullptr;
     uint32_t n = 0, n_all = 0, n_tri = 0, n_stitch = 0;
@@ -279,6 +346,22 @@ struct cc_solver {
     int lanes = 0;          // vertices are solved by groups of `lanes` threads; 0 = autotune on next step
     DBuf<double4> x_backup;
     std::vector<double> tune_ms;
+    // objective and relative residual
+    uint32_t n_hinge = 0;
+    DBuf<double4> alt;  // [n_all] second position array (fixed part = obstacle)
+    DBuf<double> gsq, term_e, partial;
+    Pinned<unsigned int> stop_h;  // two slots, one per chunk in flight
+    cudaEvent_t chunk_ev[2] = {nullptr, nullptr};
+    // learned initial guess
+    cc_mlp* mlp = nullptr;  // attached, not owned
+    int mlp_precision = 1;
+    DBuf<uint32_t> ring_off, ring, row;
+    double mean_mass = 1.0;
+    DBuf<float> feat, corr;
+    float* sample_features = nullptr;  // caller device buffers of cc_solver_step_sample
+    float* sample_targets = nullptr;
+    cudaEvent_t learn0 = nullptr, learn1 = nullptr;
+    bool learn_timed = false;
     std::string err;
     int code = 0;
     int fail(const Failure& f) {
@@ -292,6 +375,10 @@ struct cc_solver {
         if (ev1) cudaEventDestroy(ev1);
         if (tune0) cudaEventDestroy(tune0);
         if (tune1) cudaEventDestroy(tune1);
+        for (auto e : chunk_ev)
+            if (e) cudaEventDestroy(e);
+        if (learn0) cudaEventDestroy(learn0);
+        if (learn1) cudaEventDestroy(learn1);
         for (auto e : prof_events) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -363,6 +450,53 @@ struct cc_solver {
 
     void step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out);
     void autotune(const SweepView& sv);
+    ObjectiveCounts counts() const {
+        return ObjectiveCounts{n_tri, n_hinge, n_stitch, world->stats().n_contacts};
+    }
+    FeatureView feature_view(const ContactsView& cv, const cc_vbd_settings& s, double rq) {
+        FeatureView f{};
+        f.n = n;
+        f.x0 = x0.ptr;
+        f.v0 = v0.ptr;
+        f.guess = guess.ptr;
+        f.target = target.ptr;
+        f.pinned = pinned.ptr;
+        f.masses = masses.ptr;
+        f.mean_mass = mean_mass;
+        f.ring_off = ring_off.ptr;
+        f.ring = ring.ptr;
+        f.inc_off = inc_off.ptr;
+        f.inc = inc.ptr;
+        f.tri_v = tri_v.ptr;
+        f.tri_coef = tri_coef.ptr;
+        f.contacts = cv;
+        f.query_radius = rq;
+        f.relaxation = s.contact.relaxation;
+        f.dt = s.dt;
+        double g = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]);
+        f.unit = g * s.dt * s.dt > 1e-9 ? g * s.dt * s.dt : 1e-3;
+        f.row = row.ptr;
+        return f;
+    }
+    void learned_guess(const cc_vbd_settings& s, const cc_grab* grab, const ContactsView& cv, double rq,
+                       const float* features);
+    // |grad E|^2 over moving vertices at view.x into `dst` (device).
+    void grad_sq_into(const SweepView& view, double* dst) {
+        launch_grad_sq(view, gsq.ptr, nullptr, 0, lanes ? lanes : (8 | 3 << 8), stream);
+        launch_sum_partial(gsq.ptr, n, partial.ptr, nullptr, 0, stream);
+        k_store_sum<<<1, 256, 0, stream>>>(partial.ptr, dst);
+        own_launches += 3;
+    }
+    // step energy at view.x into `dst` (device).
+    void energy_into(const SweepView& view, double* dst) {
+        ObjectiveCounts c = counts();
+        uint64_t items = n + objective_items(c);
+        term_e.reserve(items);
+        launch_term_energy(view, c, term_e.ptr, stream);
+        launch_sum_partial(term_e.ptr, items, partial.ptr, nullptr, 0, stream);
+        k_store_sum<<<1, 256, 0, stream>>>(partial.ptr, dst);
+        own_launches += 3;
+    }
     void color(const ContactsView& cv, const cc_grab* grab, cc_metrics& m) {
         double t = now_ms();
         coloring.compute(color_view(cv, grab), stream);
@@ -410,6 +544,26 @@ void cc_solver::autotune(const SweepView& sv_in) {
     }
     CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
     lanes = best_g;
+}
+
+// MLP correction of the adaptive guess, clipped to the OGC balls, kept only
+// when its step energy is not higher than the adaptive guess's (the adaptive
+// warm start is already in world->x()).
+void cc_solver::learned_guess(const cc_vbd_settings& s, const cc_grab* grab, const ContactsView& cv, double rq,
+                              const float* features) {
+    if (!mlp) throw Failure{CC_ERR_INVALID_ARGUMENT, "learned initial guess requested but no MLP is attached"};
+    FeatureView f = feature_view(cv, s, rq);
+    corr.reserve((size_t)n_free * kMlpOut);
+    mlp->net->forward(features, n_free, corr.ptr, mlp_precision, stream);
+    CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_alt, 0, sizeof(unsigned int), stream));
+    launch_learned_warm_start(f, corr.ptr, alt.ptr, &sc.ptr->clipped_alt, stream);
+    SweepView sa = sweep_view(cv, s, grab);
+    energy_into(sa, &sc.ptr->e_init[0]);
+    sa.x = alt.ptr;
+    energy_into(sa, &sc.ptr->e_init[1]);
+    k_select_guess<<<grid_for(n, 256), 256, 0, stream>>>(n, alt.ptr, world->x(), sc.ptr);
+    own_launches += 3;
+    CC_CUDA(cudaGetLastError());
 }
 
 void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out) {
@@ -461,20 +615,52 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     ContactsView cv = world->contacts();
     color(cv, grab, m);
     CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
-    k_warm_start<<<gb, 256, 0, stream>>>(n, pinned.ptr, guess.ptr, cv, world->x(), sc.ptr);
+    k_warm_start<<<gb, 256, 0, stream>>>(n, pinned.ptr, guess.ptr, cv, world->x(), &sc.ptr->clipped);
     ++own_launches;
+    const bool checks = s.residual_check_every > 0 || s.residual_tolerance > 0.0;
+    const uint32_t check_every = s.residual_check_every > 0 ? s.residual_check_every : 1;
+    learn_timed = false;
+    if (s.init_mode == CC_INIT_LEARNED || sample_features) {
+        // features of the step start (the learned guess's input; training samples)
+        CC_CUDA(cudaEventRecord(learn0, stream));
+        learn_timed = true;
+        FeatureView f = feature_view(cv, s, rq);
+        float* fout = sample_features;
+        if (!fout) {
+            feat.reserve((size_t)n_free * kMlpIn);
+            fout = feat.ptr;
+        }
+        launch_features(f, fout, stream);
+        ++own_launches;
+        if (s.init_mode == CC_INIT_LEARNED) learned_guess(s, grab, cv, rq, fout);
+        CC_CUDA(cudaEventRecord(learn1, stream));
+    }
+    if (checks) {
+        // denominator |grad E(y)|^2 (alt holds y), then the initial guess's residual
+        SweepView sy = sweep_view(cv, s, grab);
+        sy.x = alt.ptr;
+        k_copy_positions<<<gb, 256, 0, stream>>>(n, target.ptr, alt.ptr);
+        ++own_launches;
+        grad_sq_into(sy, &sc.ptr->gy2);
+        grad_sq_into(sweep_view(cv, s, grab), &sc.ptr->gx2_init);
+    }
     CC_CUDA(cudaGetLastError());
     read_scalars();
     size_t clipped = sc_h.ptr->clipped;
-    // Every remaining iteration is enqueued at once; k_refresh_rule decides
-    // each refresh on the device and the host syncs once per batch, redoing
-    // from the first iteration that needed a refresh (sweeps enqueued past it
-    // exit immediately).
+    // Iterations are enqueued ahead of the device: k_refresh_rule (and, with a
+    // residual target, k_residual_rule) decide on the device and later sweeps
+    // exit at once. Without a target all iterations go in one batch and the
+    // host syncs once; with one, they go in chunks and the host reads the
+    // previous chunk's stop flag while the next chunk runs. After a refresh
+    // the host redoes detection and colouring and resumes at that iteration.
     const double threshold = s.contact.refresh_fraction * (double)n;
+    const double tol2 = s.residual_tolerance * s.residual_tolerance;
+    const bool target_on = s.residual_tolerance > 0.0;
     bool need_refresh = clipped > 0 && (double)clipped >= threshold;
     std::vector<std::pair<size_t, uint32_t>> prof_pairs;  // (event index, iteration)
     std::vector<uint32_t> prof_ok;
-    uint32_t it0 = 0;
+    uint32_t it0 = 0, executed = s.iterations;
+    CC_CUDA(cudaMemsetAsync(&sc.ptr->converged_at, 0xff, sizeof(unsigned int), stream));
     while (it0 < s.iterations) {
         if (need_refresh) {
             detect(rq, s.contact, &m, det_ms);
@@ -482,43 +668,71 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
             color(cv, grab, m);
         }
         SweepView sv = sweep_view(cv, s, grab);
-        sv.skip_at = &sc.ptr->refresh_at;
+        sv.skip_at = &sc.ptr->stop_at;
         if (lanes == 0) autotune(sv);
-        CC_CUDA(cudaMemsetAsync(&sc.ptr->refresh_at, 0xff, sizeof(unsigned int), stream));
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->refresh_at, 0xff, 2 * sizeof(unsigned int), stream));  // + converged_at
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->stop_at, 0xff, sizeof(unsigned int), stream));
         CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_iter[it0], 0, (s.iterations - it0) * sizeof(unsigned int), stream));
         const auto& off = coloring.offsets();
         size_t batch_first_pair = prof_pairs.size();
-        for (uint32_t it = it0; it < s.iterations; ++it) {
-            sv.iteration = it;
-            sv.clipped = &sc.ptr->clipped_iter[it];
-            for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
-                uint32_t cnt = off[c + 1] - off[c];
-                if (cnt == 0) continue;
-                if (profiling) {
-                    while (prof_events.size() < prof_used + 2) {
-                        cudaEvent_t e;
-                        CC_CUDA(cudaEventCreate(&e));
-                        prof_events.push_back(e);
+        const uint32_t chunk = target_on ? std::max<uint32_t>(check_every, 4) : s.iterations;
+        uint32_t chunks = 0;
+        for (uint32_t c0 = it0; c0 < s.iterations; c0 += chunk) {
+            uint32_t c1 = std::min(s.iterations, c0 + chunk);
+            for (uint32_t it = c0; it < c1; ++it) {
+                sv.iteration = it;
+                sv.clipped = &sc.ptr->clipped_iter[it];
+                for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
+                    uint32_t cnt = off[c + 1] - off[c];
+                    if (cnt == 0) continue;
+                    if (profiling) {
+                        while (prof_events.size() < prof_used + 2) {
+                            cudaEvent_t e;
+                            CC_CUDA(cudaEventCreate(&e));
+                            prof_events.push_back(e);
+                        }
+                        CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
                     }
-                    CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
+                    launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
+                    if (profiling) {
+                        CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
+                        prof_pairs.push_back({prof_used, it});
+                        prof_used += 2;
+                    }
+                    ++own_launches;
                 }
-                launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
-                if (profiling) {
-                    CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
-                    prof_pairs.push_back({prof_used, it});
-                    prof_used += 2;
-                }
+                k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold);
                 ++own_launches;
+                if (checks && ((it + 1) % check_every == 0 || it + 1 == s.iterations)) {
+                    launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, lanes, stream);
+                    launch_sum_partial(gsq.ptr, n, partial.ptr, &sc.ptr->stop_at, it, stream);
+                    k_residual_rule<<<1, 256, 0, stream>>>(sc.ptr, partial.ptr, it, s.iterations, tol2,
+                                                           target_on ? 1 : 0);
+                    own_launches += 3;
+                }
             }
-            k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold);
-            ++own_launches;
+            CC_CUDA(cudaGetLastError());
+            if (c1 >= s.iterations || !target_on) break;
+            // look ahead: enqueue the next chunk before waiting on this one's stop flag
+            unsigned int slot = chunks & 1u;
+            CC_CUDA(cudaMemcpyAsync(stop_h.ptr + slot, &sc.ptr->stop_at, sizeof(unsigned int),
+                                    cudaMemcpyDeviceToHost, stream));
+            CC_CUDA(cudaEventRecord(chunk_ev[slot], stream));
+            if (chunks > 0) {
+                CC_CUDA(cudaEventSynchronize(chunk_ev[slot ^ 1u]));
+                if (stop_h.ptr[slot ^ 1u] != 0xffffffffu) break;
+            }
+            ++chunks;
         }
-        CC_CUDA(cudaGetLastError());
         read_scalars();
-        uint32_t ra = sc_h.ptr->refresh_at;
-        uint32_t done_to = ra < s.iterations ? ra : s.iterations;
+        uint32_t ra = sc_h.ptr->refresh_at, ca = sc_h.ptr->converged_at;
+        uint32_t done_to = std::min(std::min(ra, ca), s.iterations);
         m.sweep_launches += (uint64_t)(done_to - it0) * coloring.n_colors();
         for (size_t k = batch_first_pair; k < prof_pairs.size(); ++k) prof_ok.push_back(prof_pairs[k].second < done_to);
+        if (ca <= s.iterations && ca <= ra) {
+            executed = ca;
+            break;
+        }
         if (ra < s.iterations) {
             it0 = ra;
             need_refresh = true;
@@ -526,8 +740,25 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
             it0 = s.iterations;
         }
     }
-    for (uint32_t it = 0; it < s.iterations; ++it) m.truncated_vertices += sc_h.ptr->clipped_iter[it];
-    m.vertex_solves = (uint64_t)n_free * s.iterations;
+    for (uint32_t it = 0; it < executed; ++it) m.truncated_vertices += sc_h.ptr->clipped_iter[it];
+    m.iterations = executed;
+    m.vertex_solves = (uint64_t)n_free * executed;
+    if (checks) {
+        double gy = std::sqrt(sc_h.ptr->gy2);
+        m.has_relative_residual = 1;
+        m.relative_residual = std::sqrt(sc_h.ptr->gx2) / gy;
+        m.initial_relative_residual = std::sqrt(sc_h.ptr->gx2_init) / gy;
+    }
+    m.init_used = sc_h.ptr->init_used;
+    m.init_energy_adaptive = m.init_energy_learned = std::nan("");
+    if (s.init_mode == CC_INIT_LEARNED) {
+        m.init_energy_adaptive = sc_h.ptr->e_init[0];
+        m.init_energy_learned = sc_h.ptr->e_init[1];
+    }
+    if (sample_targets) {
+        launch_targets(feature_view(cv, s, rq), world->x(), sample_targets, stream);
+        ++own_launches;
+    }
     m.colors = coloring.n_colors();
     CC_CUDA(cudaMemsetAsync(&sc.ptr->residual, 0, sizeof(double), stream));
     k_step_finish<<<gb, 256, 0, stream>>>(n, world->x(), cv, residual.ptr, sc.ptr);
@@ -607,6 +838,11 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
             sw += t;
         }
         m.sweep_ms = sw;
+    }
+    if (learn_timed) {
+        float lt = 0.f;
+        CC_CUDA(cudaEventElapsedTime(&lt, learn0, learn1));
+        m.init_ms = lt;
     }
     m.kernel_launches = own_launches + world->launches() + coloring.launches() - launches0;
     m.contact_incidence = world->stats().n_incident;
@@ -736,7 +972,7 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         std::vector<double4> tc(T);
         std::vector<double> ta(T);
         std::vector<std::vector<uint32_t>> inc(n);
-        std::vector<std::set<uint32_t>> graph(n);
+        std::vector<std::set<uint32_t>> graph(n), ring1(n);
         auto connect = [&](const uint32_t* ids, size_t k) {
             for (size_t a = 0; a < k; ++a)
                 for (size_t b = 0; b < k; ++b)
@@ -755,6 +991,9 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
             ta[t] = mesh->area[t];
             for (uint32_t k = 0; k < 3; ++k) inc[mesh->triangles[3 * t + k]].push_back(pack_term(TERM_TRI, k, (uint32_t)t));
             connect(mesh->triangles + 3 * t, 3);
+            for (uint32_t a = 0; a < 3; ++a)
+                for (uint32_t b = 0; b < 3; ++b)
+                    if (a != b) ring1[mesh->triangles[3 * t + a]].insert(mesh->triangles[3 * t + b]);
         }
         uint64_t Hn = mesh->n_hinges;
         std::vector<uint4> hv(Hn);
@@ -802,7 +1041,17 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         if (mesh->pinned)
             for (uint64_t i = 0; i < n; ++i) pin[i] = mesh->pinned[i] ? 1 : 0;
         h->n_free = 0;
-        for (uint64_t i = 0; i < n; ++i) h->n_free += pin[i] ? 0 : 1;
+        std::vector<uint32_t> rows(n, 0), rg_o(n + 1, 0), rg_v;
+        double msum = 0.0;
+        for (uint64_t i = 0; i < n; ++i) {
+            rows[i] = h->n_free;
+            h->n_free += pin[i] ? 0 : 1;
+            msum += mesh->masses[i];
+            rg_v.insert(rg_v.end(), ring1[i].begin(), ring1[i].end());
+            rg_o[i + 1] = (uint32_t)rg_v.size();
+        }
+        h->mean_mass = n ? msum / (double)n : 1.0;
+        h->n_hinge = (uint32_t)Hn;
         for (uint64_t i = 0; i < n; ++i)
             if (!(mesh->masses[i] > 0.0) || !std::isfinite(mesh->masses[i]))
                 throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
@@ -821,6 +1070,18 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         h->lo_off.upload(lo_o, st);
         h->lo.upload(lo_v, st);
         h->pinned.upload(pin, st);
+        h->row.upload(rows, st);
+        h->ring_off.upload(rg_o, st);
+        h->ring.upload(rg_v, st);
+        h->alt.reserve(n_all);
+        CC_CUDA(cudaMemcpyAsync(h->alt.ptr, h->world->x(), n_all * sizeof(double4), cudaMemcpyDeviceToDevice, st));
+        h->gsq.reserve(n);
+        h->partial.reserve(kSumBlocks);
+        h->stop_h.reserve(2);
+        CC_CUDA(cudaEventCreateWithFlags(&h->chunk_ev[0], cudaEventDisableTiming));
+        CC_CUDA(cudaEventCreateWithFlags(&h->chunk_ev[1], cudaEventDisableTiming));
+        CC_CUDA(cudaEventCreate(&h->learn0));
+        CC_CUDA(cudaEventCreate(&h->learn1));
         h->masses.upload(mesh->masses, n, st);
         for (auto* b : {&h->x0, &h->v0, &h->guess, &h->target, &h->pred_x, &h->pred_v, &h->accel}) b->reserve(n);
         h->inertia.reserve(n);
@@ -1111,6 +1372,155 @@ uint64_t cc_world_edges(const cc_world* w, uint32_t* edges_out) {
             edges_out[2 * i + 1] = e[i][1];
         }
     return e.size();
+}
+
+// ------------------------------------------------------- learned guess
+namespace {
+uint64_t mix64(uint64_t& st) {
+    uint64_t z = (st += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+}  // namespace
+
+int32_t cc_mlp_create(uint64_t seed, cc_mlp** out) {
+    try {
+        if (!out) throw Failure{CC_ERR_INVALID_ARGUMENT, "null argument"};
+        CC_CUDA(cudaSetDevice(g_device));
+        auto h = std::make_unique<cc_mlp>();
+        CC_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->net = std::make_unique<Mlp>(seed);
+        *out = h.release();
+        return CC_OK;
+    } catch (const Failure& f) {
+        return set_global(f.code, f.message);
+    }
+}
+
+void cc_mlp_destroy(cc_mlp* m) { delete m; }
+uint64_t cc_mlp_parameter_count(void) { return (uint64_t)kMlpParams; }
+
+int32_t cc_mlp_last_error(const cc_mlp* m, char* buffer, uint64_t length) {
+    copy_msg(m->err, buffer, length);
+    return m->code;
+}
+
+int32_t cc_mlp_set_parameters(cc_mlp* m, const float* params, uint64_t count) {
+    try {
+        if (!params || count != (uint64_t)kMlpParams)
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "MLP parameter count must be cc_mlp_parameter_count()"};
+        for (uint64_t i = 0; i < count; ++i)
+            if (!std::isfinite(params[i])) throw Failure{CC_ERR_INVALID_ARGUMENT, "non-finite MLP parameter"};
+        m->net->set_params(params, m->stream);
+        return CC_OK;
+    } catch (const Failure& f) {
+        return m->fail(f);
+    }
+}
+
+int32_t cc_mlp_get_parameters(cc_mlp* m, float* params, uint64_t count) {
+    try {
+        if (!params || count != (uint64_t)kMlpParams)
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "MLP parameter count must be cc_mlp_parameter_count()"};
+        m->net->get_params(params, m->stream);
+        return CC_OK;
+    } catch (const Failure& f) {
+        return m->fail(f);
+    }
+}
+
+int32_t cc_mlp_forward(cc_mlp* m, const float* features, uint64_t n, float* out, int32_t precision) {
+    try {
+        if ((n && (!features || !out)) || (precision != 0 && precision != 1))
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_mlp_forward: bad arguments"};
+        m->net->forward(features, n, out, precision, m->stream);
+        CC_CUDA(cudaStreamSynchronize(m->stream));
+        if (precision == 1 && m->net->read_error(m->stream))
+            throw Failure{CC_ERR_DEVICE_TIMEOUT, "tensor-core MLP: a bounded wait gave up"};
+        return CC_OK;
+    } catch (const Failure& f) {
+        return m->fail(f);
+    }
+}
+
+int32_t cc_mlp_gradients(cc_mlp* m, const float* features, const float* targets, uint64_t n, float* grads,
+                         float* loss) {
+    try {
+        if (!features || !targets || !grads || !loss || n == 0)
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_mlp_gradients: bad arguments"};
+        m->net->gradients(features, targets, nullptr, n, m->net->grad_buffer(), m->net->loss_buffer(), m->stream);
+        CC_CUDA(cudaMemcpyAsync(grads, m->net->grad_buffer(), kMlpParams * sizeof(float), cudaMemcpyDeviceToHost,
+                                m->stream));
+        CC_CUDA(cudaMemcpyAsync(loss, m->net->loss_buffer(), sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+        CC_CUDA(cudaStreamSynchronize(m->stream));
+        return CC_OK;
+    } catch (const Failure& f) {
+        return m->fail(f);
+    }
+}
+
+int32_t cc_mlp_train(cc_mlp* m, const float* features, const float* targets, uint64_t n, uint32_t batch,
+                     uint32_t steps, float learning_rate, uint64_t seed, float* losses) {
+    try {
+        if (!features || !targets || n == 0 || batch == 0 || steps == 0 || !(learning_rate > 0.0f))
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_mlp_train: bad arguments"};
+        if (n > 0xffffffffull) throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_mlp_train: at most 2^32-1 samples"};
+        uint64_t b = std::min<uint64_t>(batch, n);
+        m->perm.reserve(n);
+        m->losses.reserve(steps);
+        std::vector<uint32_t> perm(n);
+        for (uint64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+        uint64_t rng = seed, pos = n;  // pos = n forces a shuffle first
+        for (uint32_t t = 0; t < steps; ++t) {
+            if (pos + b > n) {  // new epoch: Fisher-Yates shuffle, upload
+                CC_CUDA(cudaStreamSynchronize(m->stream));
+                for (uint64_t i = n - 1; i > 0; --i) std::swap(perm[i], perm[mix64(rng) % (i + 1)]);
+                CC_CUDA(cudaMemcpyAsync(m->perm.ptr, perm.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                        m->stream));
+                pos = 0;
+            }
+            m->net->gradients(features, targets, m->perm.ptr + pos, b, m->net->grad_buffer(), m->losses.ptr + t,
+                              m->stream);
+            m->net->adam(m->net->grad_buffer(), learning_rate, 0.9f, 0.999f, 1e-8f, m->stream);
+            pos += b;
+        }
+        if (losses)
+            CC_CUDA(cudaMemcpyAsync(losses, m->losses.ptr, steps * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+        CC_CUDA(cudaStreamSynchronize(m->stream));
+        return CC_OK;
+    } catch (const Failure& f) {
+        return m->fail(f);
+    }
+}
+
+int32_t cc_solver_set_mlp(cc_solver* s, cc_mlp* m, int32_t precision) {
+    if (precision != 0 && precision != 1)
+        return s->fail(Failure{CC_ERR_INVALID_ARGUMENT, "MLP precision must be 0 (FP32) or 1 (FP16 tensor cores)"});
+    s->mlp = m;
+    s->mlp_precision = precision;
+    return CC_OK;
+}
+
+uint64_t cc_solver_free_vertices(const cc_solver* s) { return s->n_free; }
+
+int32_t cc_solver_step_sample(cc_solver* s, const cc_vbd_settings* settings, const cc_grab* grab, float* features,
+                              float* targets, cc_metrics* metrics) {
+    try {
+        if (!settings || !features || !targets) throw Failure{CC_ERR_INVALID_ARGUMENT, "null argument"};
+        s->sample_features = features;
+        s->sample_targets = targets;
+        try {
+            s->step(*settings, grab, metrics);
+        } catch (...) {
+            s->sample_features = s->sample_targets = nullptr;
+            throw;
+        }
+        s->sample_features = s->sample_targets = nullptr;
+        return CC_OK;
+    } catch (const Failure& f) {
+        return s->fail(f);
+    }
 }
 
 }  // extern "C"

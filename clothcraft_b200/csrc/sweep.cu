@@ -647,4 +647,112 @@ void launch_local_blocks(const SweepView& s, double* energy, double* grad, doubl
     k_local_blocks<<<grid_for(s.n, 128), 128, 0, st>>>(s, energy, grad, hess);
 }
 
+// ------------------------------------------ step objective and its gradient
+// |dE/dx_v|^2 of every moving vertex at s.x (0 where pinned): the sweep's
+// block gradient (inertia + incident terms) without an update. Skipped when
+// *skip_at <= iteration (that iteration never ran).
+template <int G>
+__global__ void __launch_bounds__(128) k_grad_sq(SweepView s, double* out, const unsigned* skip_at, uint32_t iteration) {
+    if (skip_at && *skip_at <= iteration) return;
+    uint32_t t = blockIdx.x * 128 + threadIdx.x;
+    uint32_t v = t / G;
+    if (v >= s.n) return;  // whole groups leave together
+    uint32_t lane = threadIdx.x & (G - 1);
+    unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
+    if (s.pinned[v]) {
+        if (lane == 0) out[v] = 0.0;
+        return;
+    }
+    d3 x = ld3(s.x, v);
+    d3 g = mk(0, 0, 0);
+    Sym H;
+    sym_zero(H);
+    local_part<true, G>(s, v, x, lane, g, H);
+    if (G > 1) {
+        g.x = group_sum<G>(g.x, mask);
+        g.y = group_sum<G>(g.y, mask);
+        g.z = group_sum<G>(g.z, mask);
+    }
+    g = g + (x - ld3(s.target, v)) * s.inertia[v];
+    if (lane == 0) out[v] = dot(g, g);
+}
+
+void launch_grad_sq(const SweepView& s, double* out, const unsigned* skip_at, uint32_t iteration, int variant,
+                    cudaStream_t st) {
+    int G = variant & 0xff;
+    unsigned grid = (unsigned)(((uint64_t)s.n * (uint64_t)G + 127) / 128);
+    if (grid == 0) return;
+    switch (G) {
+        case 1: k_grad_sq<1><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+        case 2: k_grad_sq<2><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+        case 4: k_grad_sq<4><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+        case 16: k_grad_sq<16><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+        case 32: k_grad_sq<32><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+        default: k_grad_sq<8><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+    }
+}
+
+// Energy of every term of the step objective, once each, at s.x:
+// [0,n) inertia of free vertices, then triangles, hinges, stitches, contacts
+// and the grab (the objective of src/solver.rs:255-296 plus the OGC terms).
+__global__ void k_term_energy(SweepView s, ObjectiveCounts c, double* out) {
+    uint64_t total = s.n + objective_items(c);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        d3 g = mk(0, 0, 0);
+        Sym H;
+        double e = 0.0;
+        uint64_t k = i;
+        if (k < s.n) {
+            if (!s.pinned[k]) {
+                d3 d = ld3(s.x, (uint32_t)k) - ld3(s.target, (uint32_t)k);
+                e = 0.5 * s.inertia[k] * dot(d, d);
+            }
+        } else if ((k -= s.n) < c.triangles) {
+            uint32_t v = (uint32_t)s.tri_v[k].x;
+            e = membrane_term<false>(s, (uint32_t)k, 0, ld3(s.x, v), g, H);
+        } else if ((k -= c.triangles) < c.hinges) {
+            uint32_t v = s.hinge_v[k].x;
+            e = bending_term<false>(s, (uint32_t)k, 0, ld3(s.x, v), g, H);
+        } else if ((k -= c.hinges) < c.stitches) {
+            uint32_t v = s.st_v[s.st_off[k]];
+            e = stitch_term<false>(s, (uint32_t)k, v, ld3(s.x, v), g, H);
+        } else if ((k -= c.stitches) < c.contacts) {
+            uint32_t v = s.contacts.verts[k].x;
+            e = contact_term<false>(s, (uint32_t)k, v, ld3(s.x, v), g, H);
+        } else if (s.grab.active) {
+            uint32_t v = s.grab.v[0];
+            e = grab_term<false>(s, v, ld3(s.x, v), g, H);
+        }
+        out[i] = e;
+    }
+}
+
+void launch_term_energy(const SweepView& s, const ObjectiveCounts& c, double* out, cudaStream_t st) {
+    uint64_t total = s.n + objective_items(c);
+    k_term_energy<<<grid_for(total, 256), 256, 0, st>>>(s, c, out);
+}
+
+// Deterministic sum, first pass: kSumBlocks fixed-order partial sums.
+__global__ void __launch_bounds__(256) k_sum_partial(const double* v, uint64_t n, double* partial,
+                                                     const unsigned* skip_at, uint32_t iteration) {
+    if (skip_at && *skip_at <= iteration) return;
+    __shared__ double sh[256];
+    double a = 0.0;
+    for (uint64_t i = blockIdx.x * 256ull + threadIdx.x; i < n; i += (uint64_t)kSumBlocks * 256ull) a += v[i];
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+void launch_sum_partial(const double* v, uint64_t n, double* partial, const unsigned* skip_at, uint32_t iteration,
+                        cudaStream_t st) {
+    k_sum_partial<<<kSumBlocks, 256, 0, st>>>(v, n, partial, skip_at, iteration);
+}
+
+
 }  // namespace cc

@@ -50,8 +50,40 @@ struct SweepView {
     unsigned char* clipped_flag;  // [n]
 };
 
+// Term counts of the step objective (k_term_energy items).
+struct ObjectiveCounts {
+    uint64_t triangles, hinges, stitches, contacts;
+};
+__host__ __device__ inline uint64_t objective_items(const ObjectiveCounts& c) {
+    return c.triangles + c.hinges + c.stitches + c.contacts + 1;  // + grab; the n vertex items come first
+}
+constexpr int kSumBlocks = 296;  // 2 x 148 SMs
+
 // launch helpers (sweep.cu)
 void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
 void launch_local_blocks(const SweepView& s, double* energy, double* grad, double* hess, cudaStream_t st);
+// out[v] = |dE/dx_v|^2 over moving vertices (variant as launch_sweep)
+void launch_grad_sq(const SweepView& s, double* out, const unsigned* skip_at, uint32_t iteration, int variant,
+                    cudaStream_t st);
+// out[i] = energy of objective item i; items = s.n + objective_items(c)
+void launch_term_energy(const SweepView& s, const ObjectiveCounts& c, double* out, cudaStream_t st);
+void launch_sum_partial(const double* v, uint64_t n, double* partial, const unsigned* skip_at, uint32_t iteration,
+                        cudaStream_t st);
+// Second pass of the deterministic sum, run by one block of 256 threads: the
+// kSumBlocks partials added in a fixed order (valid in every thread).
+__device__ __forceinline__ double block_sum_partials(const double* partial) {
+    __shared__ double sh[256];
+    double a = 0.0;
+    for (int i = threadIdx.x; i < kSumBlocks; i += 256) a += partial[i];
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
 
 }  // namespace cc

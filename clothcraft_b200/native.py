@@ -51,6 +51,21 @@ SIGNATURES = {
                                     C.POINTER(cc_contacts)]),
     "cc_world_candidates": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_candidates)]),
     "cc_world_edges": (C.c_uint64, [C.c_void_p, c_uint32_p]),
+    "cc_mlp_create": (C.c_int32, [C.c_uint64, C.POINTER(C.c_void_p)]),
+    "cc_mlp_destroy": (None, [C.c_void_p]),
+    "cc_mlp_last_error": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_uint64]),
+    "cc_mlp_parameter_count": (C.c_uint64, []),
+    "cc_mlp_set_parameters": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_uint64]),
+    "cc_mlp_get_parameters": (C.c_int32, [C.c_void_p, C.POINTER(C.c_float), C.c_uint64]),
+    "cc_mlp_forward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_int32]),
+    "cc_mlp_gradients": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float)]),
+    "cc_mlp_train": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_uint32,
+                                 C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "cc_solver_set_mlp": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32]),
+    "cc_solver_free_vertices": (C.c_uint64, [C.c_void_p]),
+    "cc_solver_step_sample": (C.c_int32, [C.c_void_p, C.POINTER(cc_vbd_settings), C.POINTER(cc_grab), C.c_void_p,
+                                          C.c_void_p, C.POINTER(cc_metrics)]),
     "cc_ogc_radii_noalloc": (C.c_int32, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,
                                          C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64, C.c_double,
                                          C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),

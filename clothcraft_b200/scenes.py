@@ -352,11 +352,17 @@ class StepSettings:
     stiffness: float = 100000.0
     relaxation: float = 0.45
     refresh_fraction: float = 0.01
+    init_mode: int = 0  # 0 adaptive (reference), 1 learned
+    residual_tolerance: float = 0.0
+    residual_check_every: int = 0
 
     def to_c(self) -> abi.cc_vbd_settings:
         s = abi.cc_vbd_settings()
         s.dt = self.dt
         s.iterations = self.iterations
+        s.init_mode = self.init_mode
+        s.residual_tolerance = self.residual_tolerance
+        s.residual_check_every = self.residual_check_every
         s.damping = self.damping
         for k in range(3):
             s.gravity[k] = self.gravity[k]

@@ -204,6 +204,38 @@ class VbdSolver:
             raise self._err(rc)
         return x, v, t.value
 
+    # learned initial guess
+    def set_mlp(self, mlp, precision=1):
+        """Attach an Mlp (clothcraft_b200.learned.Mlp) for init_mode = 1;
+        precision 0 = FP32 CUDA cores, 1 = FP16 tensor cores. None detaches."""
+        self._mlp = mlp  # keep the network alive while attached
+        rc = native.load().cc_solver_set_mlp(self.h, None if mlp is None else mlp.h, int(precision))
+        if rc != 0:
+            raise self._err(rc)
+
+    @property
+    def free_vertices(self) -> int:
+        return int(native.load().cc_solver_free_vertices(self.h))
+
+    def step_sample(self, settings, features, targets, grab=None):
+        """step_resident that also writes the step's training sample into the
+        CUDA float32 tensors features [free, 24] and targets [free, 3]."""
+        import torch
+
+        rows = self.free_vertices
+        for t, w in ((features, 24), (targets, 3)):
+            if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous() and tuple(t.shape) == (rows, w)):
+                raise ValueError("sample buffers must be contiguous CUDA float32 [%d, %d]" % (rows, w))
+        torch.cuda.synchronize()
+        m = cc_metrics()
+        s = _settings_c(settings)
+        g = _grab_c(grab)
+        rc = native.load().cc_solver_step_sample(self.h, C.byref(s), _ref(g, cc_grab), C.c_void_p(features.data_ptr()),
+                                                 C.c_void_p(targets.data_ptr()), C.byref(m))
+        if rc != 0:
+            raise self._err(rc)
+        return m.as_dict()
+
     def step_resident(self, settings, grab=None):
         m = cc_metrics()
         s = _settings_c(settings)

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define CC_ABI_VERSION 1
+#define CC_ABI_VERSION 2
 
 enum cc_status {
     CC_OK = 0,
@@ -95,14 +95,34 @@ typedef struct cc_ogc_settings {
     double refresh_fraction;
 } cc_ogc_settings;
 
-/* VbdSettings (src/vbd.rs:18-52). */
+/* Initial guess of the sweeps. */
+enum cc_init_mode {
+    CC_INIT_ADAPTIVE = 0, /* Prediction::guess (src/vbd/prediction.rs:15-41) */
+    CC_INIT_LEARNED = 1   /* MLP correction of the adaptive guess, kept only */
+                          /* when its step energy is not higher (cc_mlp_*)   */
+};
+/* VbdSettings (src/vbd.rs:18-52), plus two extensions without a reference
+ * counterpart: the initial-guess mode and a relative-residual target.
+ *
+ * relative residual = ||grad E(x)|| / ||grad E(y)|| over free vertices, E the
+ * step objective (inertia + membrane + bending + stitches + grab + OGC
+ * terms), y the inertial target.
+ * The OGC terms are those in force when the residual is evaluated (the
+ * step's detection, or its latest refresh).
+ * residual_check_every = 0: never evaluated (the reference's behaviour).
+ * residual_check_every = k > 0: evaluated after every k-th iteration and
+ * after the last; with residual_tolerance > 0 the iterations stop at the
+ * first evaluation <= residual_tolerance (`iterations` is then the cap). */
 typedef struct cc_vbd_settings {
     double dt;
     uint32_t iterations;
-    uint32_t reserved0;
+    uint32_t init_mode;              /* cc_init_mode                        */
     double damping;
     double gravity[3];
     cc_ogc_settings contact;
+    double residual_tolerance;       /* 0 = run all `iterations`            */
+    uint32_t residual_check_every;   /* 0 = no relative residual            */
+    uint32_t reserved0;
 } cc_vbd_settings;
 
 /* Grab (src/vbd.rs:54-60): mouse attachment, weights sum to one. */
@@ -136,6 +156,15 @@ typedef struct cc_metrics {
     uint64_t contact_incidence;     /* entries of the last contact incidence  */
     double color_ms;                /* host time spent colouring              */
     uint64_t color_rounds;          /* greedy-rule rounds of the colourings   */
+    /* relative residual (see cc_vbd_settings) after the last iteration and
+     * of the initial guess; defined when has_relative_residual = 1 */
+    double relative_residual;
+    double initial_relative_residual;
+    int32_t has_relative_residual;
+    int32_t init_used;              /* cc_init_mode the sweeps started from   */
+    double init_energy_adaptive;    /* step energy of the two initial guesses */
+    double init_energy_learned;     /* (learned mode; NaN otherwise)          */
+    double init_ms;                 /* device time of the learned guess       */
 } cc_metrics;
 
 /* ContactSet (src/ogc/world.rs:73-107) in caller-owned arrays. The contact
@@ -272,6 +301,51 @@ int32_t cc_world_candidates(cc_world* world, const double* x, double radius,
 /* Topology sizes: edges of the combined mesh (src/ogc/topology.rs:13-52). */
 uint64_t cc_world_edges(const cc_world* world, uint32_t* edges_out);
 
+/* ------------------------------------------------------ learned guess */
+/* No reference counterpart. A 24-64-64-64-3 GELU MLP predicts, per free
+ * vertex, a correction of the adaptive guess from 24 features of the step
+ * start (inertial and previous displacement, neighbourhood, local strain,
+ * nearest-contact distance). With init_mode = CC_INIT_LEARNED the solver
+ * clips the learned guess to the OGC balls (ContactSet::truncate,
+ * src/ogc/world.rs:91-100) and keeps it only when its step energy is not
+ * higher than the adaptive guess's; cc_metrics.init_used says which one ran.
+ *
+ * Arrays marked (device) are device pointers; the calls synchronise their
+ * own stream before returning and expect the buffers to be ready. */
+typedef struct cc_mlp cc_mlp;
+/* New network, Glorot-uniform weights from `seed`, zero biases. */
+int32_t cc_mlp_create(uint64_t seed, cc_mlp** out);
+void cc_mlp_destroy(cc_mlp* mlp);
+int32_t cc_mlp_last_error(const cc_mlp* mlp, char* buffer, uint64_t length);
+/* Parameters (float32, host): W1[64][24] b1[64] W2[64][64] b2[64] W3[64][64]
+ * b3[64] W4[3][64] b4[3], W[out][in]; count = cc_mlp_parameter_count(). */
+uint64_t cc_mlp_parameter_count(void);
+int32_t cc_mlp_set_parameters(cc_mlp* mlp, const float* params, uint64_t count);
+int32_t cc_mlp_get_parameters(cc_mlp* mlp, float* params, uint64_t count);
+/* out (device) [n][3] = MLP(features (device) [n][24]); precision 0 = FP32
+ * CUDA cores, 1 = FP16 operands / FP32 accumulation on the tensor cores. */
+int32_t cc_mlp_forward(cc_mlp* mlp, const float* features, uint64_t n, float* out, int32_t precision);
+/* Gradient (host, [count]) and value (host) of the loss
+ * L = (1/n) sum_s |MLP(features_s) - targets_s|^2 (device inputs). */
+int32_t cc_mlp_gradients(cc_mlp* mlp, const float* features, const float* targets, uint64_t n,
+                         float* grads, float* loss);
+/* `steps` Adam steps (beta 0.9/0.999, eps 1e-8) on minibatches of `batch`
+ * samples drawn without replacement per epoch (seeded shuffle); losses
+ * (host, [steps], may be NULL) receives each minibatch's loss. */
+int32_t cc_mlp_train(cc_mlp* mlp, const float* features, const float* targets, uint64_t n,
+                     uint32_t batch, uint32_t steps, float learning_rate, uint64_t seed, float* losses);
+/* Attach a network to a solver (not owned; NULL detaches). precision as in
+ * cc_mlp_forward. */
+int32_t cc_solver_set_mlp(cc_solver* solver, cc_mlp* mlp, int32_t precision);
+/* Rows of the training arrays: the solver's free (unpinned) vertices. */
+uint64_t cc_solver_free_vertices(const cc_solver* solver);
+/* cc_solver_step_resident that also writes one training sample per free
+ * vertex, in vertex order: features (device) [rows][24] of the step start and
+ * targets (device) [rows][3] = (x_end - adaptive guess) / (|g| dt^2), the
+ * correction the network should have predicted for this step's result. */
+int32_t cc_solver_step_sample(cc_solver* solver, const cc_vbd_settings* settings,
+                              const cc_grab* grab, float* features, float* targets,
+                              cc_metrics* metrics);
 /* ------------------------------------------------------- allocation-free */
 /* No counterpart in the reference. Per-vertex OGC distances and conservative
  * radii for given candidate pairs, without allocating any memory, for callers

@@ -97,6 +97,12 @@ def lib():
                                            C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "or_step_gradient": (C.c_int32, [vp, c_double_p, c_double_p, C.POINTER(cc_vbd_settings), c_double_p,
                                              C.c_int32, c_double_p, c_double_p]),
+            "or_mlp_parameter_count": (C.c_uint64, []),
+            "or_mlp_forward": (C.c_int32, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_uint64, c_double_p]),
+            "or_mlp_gradients": (C.c_int32, [C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                             C.c_uint64, c_double_p, c_double_p]),
+            "or_learned_features": (C.c_int32, [vp, c_double_p, c_double_p, C.c_double, C.POINTER(cc_vbd_settings),
+                                                C.POINTER(C.c_float)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -234,6 +240,7 @@ class Solver:
         self.n = scene.n
         self.total = int(L.or_solver_total(h))
         self.obstacle_x = None if scene.obstacle is None else abi.as_f64(scene.obstacle.vertices)
+        self._pinned = np.asarray(scene.mesh.pinned).astype(bool)
         L.or_set_threads(h, int(threads))
         self.world = World(None, None, self.n, _handle=L.or_solver_world(h), _owner=self)
 
@@ -283,6 +290,21 @@ class Solver:
         if rc != 0:
             raise OracleError(rc, "Newton step failed")
         return out, res.value, bool(conv.value), its.value
+
+    def learned_features(self, x, v, time, settings: cc_vbd_settings):
+        """The 24 learned-guess features of the step starting at (x, v, time)
+        with this solver's prediction history; [free vertices, 24] float32."""
+        x = abi.as_f64(x)
+        v = abi.as_f64(v)
+        rows = int(np.count_nonzero(~self._pinned)) if hasattr(self, "_pinned") else None
+        if rows is None:
+            raise OracleError(1, "solver built without pin information")
+        out = np.zeros((rows, 24), np.float32)
+        rc = lib().or_learned_features(self.h, f64p(x), f64p(v), float(time), C.byref(settings),
+                                       out.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc != 0:
+            raise OracleError(rc, "feature evaluation failed")
+        return out
 
     def step_gradient(self, x_old, v_old, settings: cc_vbd_settings, x_eval, threads=8):
         """Objective and gradient (pinned dofs zero) of the step from
@@ -367,3 +389,27 @@ class Bvh:
         b = abi.as_f64(box6)
         k = lib().or_bvh_query(self.h, f64p(b), int(dynamic_only), u32p(out), cap)
         return out[:k].copy()
+
+
+def mlp_forward(params, features):
+    """FP64 forward of the 24-64-64-64-3 GELU MLP (parameters and features float32)."""
+    p = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(features, np.float32)
+    out = np.zeros((f.shape[0], 3))
+    lib().or_mlp_forward(p.ctypes.data_as(C.POINTER(C.c_float)), f.ctypes.data_as(C.POINTER(C.c_float)), f.shape[0],
+                         f64p(out))
+    return out
+
+
+def mlp_gradients(params, features, targets):
+    """FP64 gradient and value of mean_s |MLP(f_s) - t_s|^2."""
+    p = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(features, np.float32)
+    t = np.ascontiguousarray(targets, np.float32)
+    g = np.zeros(p.size)
+    loss = C.c_double()
+    rc = lib().or_mlp_gradients(p.ctypes.data_as(C.POINTER(C.c_float)), f.ctypes.data_as(C.POINTER(C.c_float)),
+                                t.ctypes.data_as(C.POINTER(C.c_float)), f.shape[0], f64p(g), C.byref(loss))
+    if rc != 0:
+        raise OracleError(rc, "MLP gradient failed")
+    return g, loss.value

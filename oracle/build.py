@@ -12,7 +12,7 @@ import subprocess
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-SOURCES = ["oracle_ogc.cpp", "oracle_vbd.cpp", "oracle_capi.cpp", "oracle_newton.cpp"]
+SOURCES = ["oracle_ogc.cpp", "oracle_vbd.cpp", "oracle_capi.cpp", "oracle_newton.cpp", "oracle_learned.cpp"]
 OUT = HERE / "_build" / "liboracle.so"
 
 
