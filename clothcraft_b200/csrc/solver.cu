@@ -78,8 +78,12 @@ struct StepScalars {
     double gy2;        // |grad E(y)|^2, y the inertial target
     double gx2;        // |grad E(x)|^2 at the last evaluation
     double gx2_init;   // |grad E|^2 of the initial guess
-    double e_init[2];  // step energy of the adaptive / learned initial guess
+    double e_init[2];  // step energy of the adaptive / full-scale learned guess
     int init_used;
+    double gx2_iter[256];   // |P grad E(x)|^2 after iteration it (evaluated ones)
+    double e_cand, best_e;  // learned-guess scale search
+    unsigned int clipped_best;
+    int take;
 };
 
 __global__ void k_step_begin(uint32_t n, const double4* x0, const double4* v0, const double4* px, const double4* pv,
@@ -174,6 +178,7 @@ __global__ void __launch_bounds__(256) k_residual_rule(StepScalars* sc, const do
     double g2 = block_sum_partials(partial);
     if (threadIdx.x == 0) {
         sc->gx2 = g2;
+        sc->gx2_iter[it] = g2;
         sc->checked_at = it + 1;
         if (stop && g2 <= tol2 * sc->gy2 && sc->converged_at > it + 1) {
             sc->converged_at = it + 1;
@@ -481,8 +486,8 @@ struct cc_solver {
     void learned_guess(const cc_vbd_settings& s, const cc_grab* grab, const ContactsView& cv, double rq,
                        const float* features);
     // |grad E|^2 over moving vertices at view.x into `dst` (device).
-    void grad_sq_into(const SweepView& view, double* dst) {
-        launch_grad_sq(view, gsq.ptr, nullptr, 0, lanes ? lanes : (8 | 3 << 8), stream);
+    void grad_sq_into(const SweepView& view, double* dst, bool project) {
+        launch_grad_sq(view, gsq.ptr, nullptr, 0, lanes ? lanes : (8 | 3 << 8), project, stream);
         launch_sum_partial(gsq.ptr, n, partial.ptr, nullptr, 0, stream);
         k_store_sum<<<1, 256, 0, stream>>>(partial.ptr, dst);
         own_launches += 3;
@@ -509,8 +514,8 @@ struct cc_solver {
 // a backup of the positions (restored after each trial) and keep the fastest.
 void cc_solver::autotune(const SweepView& sv_in) {
     // lanes per vertex | register cap (3 or 4 resident 128-thread blocks per SM) << 8
-    static const int kCandidates[] = {1 | 3 << 8, 2 | 3 << 8,  4 | 3 << 8,  4 | 4 << 8, 8 | 3 << 8,
-                                      8 | 4 << 8, 16 | 3 << 8, 16 | 4 << 8, 32 | 3 << 8};
+    static const int kCandidates[] = {1 | 3 << 8, 2 | 3 << 8, 4 | 3 << 8,  4 | 4 << 8,  4 | 5 << 8, 8 | 3 << 8,
+                                      8 | 4 << 8, 8 | 5 << 8, 16 | 3 << 8, 16 | 4 << 8, 32 | 3 << 8};
     SweepView sv = sv_in;  // trial sweeps never skip and count into a scratch counter
     sv.skip_at = nullptr;
     sv.clipped = &sc.ptr->clipped;
@@ -641,8 +646,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         sy.x = alt.ptr;
         k_copy_positions<<<gb, 256, 0, stream>>>(n, target.ptr, alt.ptr);
         ++own_launches;
-        grad_sq_into(sy, &sc.ptr->gy2);
-        grad_sq_into(sweep_view(cv, s, grab), &sc.ptr->gx2_init);
+        grad_sq_into(sy, &sc.ptr->gy2, false);
+        grad_sq_into(sweep_view(cv, s, grab), &sc.ptr->gx2_init, true);
     }
     CC_CUDA(cudaGetLastError());
     read_scalars();
@@ -661,6 +666,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     std::vector<uint32_t> prof_ok;
     uint32_t it0 = 0, executed = s.iterations;
     CC_CUDA(cudaMemsetAsync(&sc.ptr->converged_at, 0xff, sizeof(unsigned int), stream));
+    if (checks) CC_CUDA(cudaMemsetAsync(sc.ptr->gx2_iter, 0xff, sizeof(sc.ptr->gx2_iter), stream));  // NaN: not evaluated
     while (it0 < s.iterations) {
         if (need_refresh) {
             detect(rq, s.contact, &m, det_ms);
@@ -704,7 +710,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                 k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold);
                 ++own_launches;
                 if (checks && ((it + 1) % check_every == 0 || it + 1 == s.iterations)) {
-                    launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, lanes, stream);
+                    launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, lanes, true, stream);
                     launch_sum_partial(gsq.ptr, n, partial.ptr, &sc.ptr->stop_at, it, stream);
                     k_residual_rule<<<1, 256, 0, stream>>>(sc.ptr, partial.ptr, it, s.iterations, tol2,
                                                            target_on ? 1 : 0);
@@ -1503,6 +1509,18 @@ int32_t cc_solver_set_mlp(cc_solver* s, cc_mlp* m, int32_t precision) {
 }
 
 uint64_t cc_solver_free_vertices(const cc_solver* s) { return s->n_free; }
+
+int32_t cc_solver_last_step_trace(const cc_solver* s, double* relative_residual, uint32_t* clipped,
+                                  uint32_t capacity) {
+    uint32_t k = std::min<uint32_t>(capacity, 256u);
+    double gy2 = s->sc_h.ptr->gy2;
+    for (uint32_t i = 0; i < k; ++i) {
+        double g = s->sc_h.ptr->gx2_iter[i];
+        if (relative_residual) relative_residual[i] = std::isnan(g) ? g : std::sqrt(g / gy2);
+        if (clipped) clipped[i] = s->sc_h.ptr->clipped_iter[i];
+    }
+    return CC_OK;
+}
 
 int32_t cc_solver_step_sample(cc_solver* s, const cc_vbd_settings* settings, const cc_grab* grab, float* features,
                               float* targets, cc_metrics* metrics) {

@@ -595,7 +595,8 @@ static void launch_g(const SweepView& s, const uint32_t* order, uint32_t count, 
     constexpr int B = 128;
     uint64_t threads = (uint64_t)count * G;
     unsigned grid = (unsigned)((threads + B - 1) / B);
-    if (minb >= 4) k_sweep<G, B, 4><<<grid, B, 0, st>>>(s, order, count);
+    if (minb >= 5) k_sweep<G, B, 5><<<grid, B, 0, st>>>(s, order, count);
+    else if (minb == 4) k_sweep<G, B, 4><<<grid, B, 0, st>>>(s, order, count);
     else k_sweep<G, B, 3><<<grid, B, 0, st>>>(s, order, count);
 }
 
@@ -649,10 +650,15 @@ void launch_local_blocks(const SweepView& s, double* energy, double* grad, doubl
 
 // ------------------------------------------ step objective and its gradient
 // |dE/dx_v|^2 of every moving vertex at s.x (0 where pinned): the sweep's
-// block gradient (inertia + incident terms) without an update. Skipped when
+// block gradient (inertia + incident terms) without an update. With
+// `project`, a vertex on the boundary of its OGC ball (|x - c| >= b) whose
+// descent direction -g points out of the ball keeps only the tangential part
+// of g: the first-order (KKT) residual of the step's ball-constrained
+// problem (ContactSet::truncate, src/ogc/world.rs:91-100). Skipped when
 // *skip_at <= iteration (that iteration never ran).
 template <int G>
-__global__ void __launch_bounds__(128) k_grad_sq(SweepView s, double* out, const unsigned* skip_at, uint32_t iteration) {
+__global__ void __launch_bounds__(128) k_grad_sq(SweepView s, double* out, const unsigned* skip_at, uint32_t iteration,
+                                                 int project) {
     if (skip_at && *skip_at <= iteration) return;
     uint32_t t = blockIdx.x * 128 + threadIdx.x;
     uint32_t v = t / G;
@@ -674,21 +680,28 @@ __global__ void __launch_bounds__(128) k_grad_sq(SweepView s, double* out, const
         g.z = group_sum<G>(g.z, mask);
     }
     g = g + (x - ld3(s.target, v)) * s.inertia[v];
+    if (project) {
+        d3 d = x - ld3(s.contacts.centers, v);
+        double l = len(d), b = s.contacts.radii[v];
+        double gn = dot(g, d);
+        if (l >= b * (1.0 - 1e-9) && l > 0.0 && gn < 0.0) g = g - d * (gn / (l * l));
+    }
     if (lane == 0) out[v] = dot(g, g);
 }
 
 void launch_grad_sq(const SweepView& s, double* out, const unsigned* skip_at, uint32_t iteration, int variant,
-                    cudaStream_t st) {
+                    bool project, cudaStream_t st) {
     int G = variant & 0xff;
     unsigned grid = (unsigned)(((uint64_t)s.n * (uint64_t)G + 127) / 128);
     if (grid == 0) return;
+    int p = project ? 1 : 0;
     switch (G) {
-        case 1: k_grad_sq<1><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
-        case 2: k_grad_sq<2><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
-        case 4: k_grad_sq<4><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
-        case 16: k_grad_sq<16><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
-        case 32: k_grad_sq<32><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
-        default: k_grad_sq<8><<<grid, 128, 0, st>>>(s, out, skip_at, iteration); break;
+        case 1: k_grad_sq<1><<<grid, 128, 0, st>>>(s, out, skip_at, iteration, p); break;
+        case 2: k_grad_sq<2><<<grid, 128, 0, st>>>(s, out, skip_at, iteration, p); break;
+        case 4: k_grad_sq<4><<<grid, 128, 0, st>>>(s, out, skip_at, iteration, p); break;
+        case 16: k_grad_sq<16><<<grid, 128, 0, st>>>(s, out, skip_at, iteration, p); break;
+        case 32: k_grad_sq<32><<<grid, 128, 0, st>>>(s, out, skip_at, iteration, p); break;
+        default: k_grad_sq<8><<<grid, 128, 0, st>>>(s, out, skip_at, iteration, p); break;
     }
 }
 

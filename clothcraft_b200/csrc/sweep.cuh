@@ -62,9 +62,10 @@ constexpr int kSumBlocks = 296;  // 2 x 148 SMs
 // launch helpers (sweep.cu)
 void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
 void launch_local_blocks(const SweepView& s, double* energy, double* grad, double* hess, cudaStream_t st);
-// out[v] = |dE/dx_v|^2 over moving vertices (variant as launch_sweep)
+// out[v] = |dE/dx_v|^2 over moving vertices (variant as launch_sweep); with
+// `project`, the KKT residual of the OGC-ball constraints (sweep.cu)
 void launch_grad_sq(const SweepView& s, double* out, const unsigned* skip_at, uint32_t iteration, int variant,
-                    cudaStream_t st);
+                    bool project, cudaStream_t st);
 // out[i] = energy of objective item i; items = s.n + objective_items(c)
 void launch_term_energy(const SweepView& s, const ObjectiveCounts& c, double* out, cudaStream_t st);
 void launch_sum_partial(const double* v, uint64_t n, double* partial, const unsigned* skip_at, uint32_t iteration,

@@ -64,6 +64,7 @@ SIGNATURES = {
                                  C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "cc_solver_set_mlp": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32]),
     "cc_solver_free_vertices": (C.c_uint64, [C.c_void_p]),
+    "cc_solver_last_step_trace": (C.c_int32, [C.c_void_p, c_double_p, c_uint32_p, C.c_uint32]),
     "cc_solver_step_sample": (C.c_int32, [C.c_void_p, C.POINTER(cc_vbd_settings), C.POINTER(cc_grab), C.c_void_p,
                                           C.c_void_p, C.POINTER(cc_metrics)]),
     "cc_ogc_radii_noalloc": (C.c_int32, [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p, C.c_uint64, C.c_void_p,

@@ -213,6 +213,14 @@ class VbdSolver:
         if rc != 0:
             raise self._err(rc)
 
+    def last_step_trace(self):
+        """(relative residual after each iteration, NaN where not evaluated;
+        vertices clipped in each iteration) of the last step."""
+        r = np.zeros(256)
+        c = np.zeros(256, np.uint32)
+        native.load().cc_solver_last_step_trace(self.h, _f64p(r), _u32p(c), 256)
+        return r, c
+
     @property
     def free_vertices(self) -> int:
         return int(native.load().cc_solver_free_vertices(self.h))

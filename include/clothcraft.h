@@ -104,9 +104,13 @@ enum cc_init_mode {
 /* VbdSettings (src/vbd.rs:18-52), plus two extensions without a reference
  * counterpart: the initial-guess mode and a relative-residual target.
  *
- * relative residual = ||grad E(x)|| / ||grad E(y)|| over free vertices, E the
- * step objective (inertia + membrane + bending + stitches + grab + OGC
- * terms), y the inertial target.
+ * relative residual = ||P grad E(x)|| / ||grad E(y)|| over free vertices, E
+ * the step objective (inertia + membrane + bending + stitches + grab + OGC
+ * terms), y the inertial target, P the projection that drops the outward
+ * normal part of a vertex's gradient when the vertex sits on the boundary of
+ * its OGC ball and its descent direction leaves the ball: the first-order
+ * residual of the ball-constrained problem the sweeps solve (without P the
+ * norm stalls at the forces the trust region holds back).
  * The OGC terms are those in force when the residual is evaluated (the
  * step's detection, or its latest refresh).
  * residual_check_every = 0: never evaluated (the reference's behaviour).
@@ -337,6 +341,12 @@ int32_t cc_mlp_train(cc_mlp* mlp, const float* features, const float* targets, u
 /* Attach a network to a solver (not owned; NULL detaches). precision as in
  * cc_mlp_forward. */
 int32_t cc_solver_set_mlp(cc_solver* solver, cc_mlp* mlp, int32_t precision);
+/* Per-iteration record of the last step (no reference counterpart), for
+ * convergence studies: relative residual after each iteration (NaN where it
+ * was not evaluated) and vertices clipped to their OGC balls in it; entries
+ * up to min(capacity, 256). */
+int32_t cc_solver_last_step_trace(const cc_solver* solver, double* relative_residual,
+                                  uint32_t* clipped, uint32_t capacity);
 /* Rows of the training arrays: the solver's free (unpinned) vertices. */
 uint64_t cc_solver_free_vertices(const cc_solver* solver);
 /* cc_solver_step_resident that also writes one training sample per free

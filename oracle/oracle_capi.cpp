@@ -54,6 +54,8 @@ VbdSettings to_vbd(const cc_vbd_settings* s) {
     o.damping = s->damping;
     o.gravity = {s->gravity[0], s->gravity[1], s->gravity[2]};
     o.contact = to_ogc(&s->contact);
+    o.residual_tolerance = s->residual_tolerance;
+    o.residual_check_every = s->residual_check_every;
     return o;
 }
 
@@ -146,6 +148,9 @@ void fill_metrics(const VbdMetrics& m, cc_metrics* out) {
     out->extension_max_percent = m.extension_max_percent;
     out->residual_rms_n = m.residual_rms_n;
     out->has_residual = m.has_residual ? 1 : 0;
+    out->has_relative_residual = m.has_relative_residual ? 1 : 0;
+    out->relative_residual = m.relative_residual;
+    out->initial_relative_residual = m.initial_relative_residual;
 }
 
 int fill_contacts(const ContactSet& cs, size_t moving, cc_contacts* out) {

@@ -186,6 +186,34 @@ struct Update {
 }  // namespace
 
 // src/vbd.rs:250-422
+// With `project`, a vertex on the boundary of its OGC ball whose descent
+// direction points out of the ball keeps the tangential part of its gradient
+// only (first-order residual of the ball-constrained step, ContactSet::truncate).
+double VbdSolver::grad_sq(const std::vector<D3>& x, const ContactSet& contacts, const std::vector<D3>& target,
+                          const std::vector<double>& inertia, const VbdSettings& settings, const Grab* grab,
+                          bool project) const {
+    const size_t n = mesh.n;
+    std::vector<double> g2(n, 0.0);
+#pragma omp parallel for num_threads(threads) schedule(dynamic, 64)
+    for (size_t v = 0; v < n; ++v) {
+        if (mesh.pinned[v]) continue;
+        V3<Jet<3>> p;
+        for (int k = 0; k < 3; ++k) p[k] = variable<3>(x[v][k], k);
+        Jet<3> jet = local<Jet<3>>((uint32_t)v, p, x, contacts, settings, grab);
+        D3 g = D3{jet.g[0], jet.g[1], jet.g[2]} + (x[v] - target[v]) * inertia[v];
+        if (project) {
+            D3 d = x[v] - contacts.centers[v];
+            double l = length(d), b = contacts.radii[v];
+            double gn = dot(g, d);
+            if (l >= b * (1.0 - 1e-9) && l > 0.0 && gn < 0.0) g = g - d * (gn / (l * l));
+        }
+        g2[v] = length_squared(g);
+    }
+    double s = 0.0;
+    for (double a : g2) s += a;
+    return s;
+}
+
 VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab* grab) {
     if (!settings.valid()) throw Error{1, "Invalid VBD settings"};
     const size_t n = mesh.n;
@@ -242,6 +270,16 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
             x[i] = contacts.truncate(i, guess[i], b);
             clipped += b ? 1 : 0;
         }
+    }
+    const bool checks = settings.residual_check_every > 0 || settings.residual_tolerance > 0.0;
+    const size_t check_every = settings.residual_check_every > 0 ? settings.residual_check_every : 1;
+    double gy2 = 0.0;
+    if (checks) {
+        std::vector<D3> y_all = world.positions(target.data(), n);
+        gy2 = grad_sq(y_all, contacts, target, inertia, settings, grab, false);
+        metrics.initial_relative_residual =
+            std::sqrt(grad_sq(x, contacts, target, inertia, settings, grab, true) / gy2);
+        metrics.has_relative_residual = true;
     }
     std::vector<Update> updates;
     for (size_t it = 0; it < settings.iterations; ++it) {
@@ -310,6 +348,15 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
         metrics.residual_rms_n = std::sqrt(residual / (double)(3 * n));
         metrics.has_residual = true;
         metrics.colors = colors.size();
+        if (checks && ((it + 1) % check_every == 0 || it + 1 == settings.iterations)) {
+            double gx2 = grad_sq(x, contacts, target, inertia, settings, grab, true);
+            metrics.relative_residual = std::sqrt(gx2 / gy2);
+            if (settings.residual_tolerance > 0.0 &&
+                gx2 <= settings.residual_tolerance * settings.residual_tolerance * gy2) {
+                metrics.iterations = it + 1;
+                break;
+            }
+        }
     }
     for (const auto& p : x)
         if (!finite(p)) throw Error{4, "Non-finite VBD result; state unchanged"};

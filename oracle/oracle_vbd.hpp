@@ -42,6 +42,11 @@ struct VbdSettings {  // src/vbd.rs:18-52
     double damping = 1.5;
     D3 gravity{0.0, -9.81, 0.0};
     OgcSettings contact;
+    // Extension without a reference counterpart (the library's residual
+    // target): evaluate ||P grad E(x)|| / ||grad E(y)|| every k iterations and
+    // stop at the first evaluation <= tolerance (0 = never stop early).
+    double residual_tolerance = 0.0;
+    size_t residual_check_every = 0;
     bool valid() const;
 };
 
@@ -61,6 +66,8 @@ struct VbdMetrics {  // src/vbd.rs:61-83
     double minimum_distance_m = 0, max_seam_gap_m = 0, extension_p95_percent = 0, extension_max_percent = 0;
     bool has_residual = false;
     double residual_rms_n = 0;
+    bool has_relative_residual = false;
+    double relative_residual = 0, initial_relative_residual = 0;
 };
 
 struct State {
@@ -92,6 +99,11 @@ struct VbdSolver {  // src/vbd.rs:89-99
     S local(uint32_t v, const V3<S>& p, const std::vector<D3>& x, const ContactSet& contact, const VbdSettings& s,
             const Grab* grab) const;
     VbdMetrics step(State& state, const VbdSettings& settings, const Grab* grab);
+    // sum over free vertices of |dE/dx_v|^2 at positions x (all vertices);
+    // with `project`, the ball-constraint KKT residual (see grad_sq)
+    double grad_sq(const std::vector<D3>& x, const ContactSet& contacts, const std::vector<D3>& target,
+                   const std::vector<double>& inertia, const VbdSettings& settings, const Grab* grab,
+                   bool project) const;
 };
 
 // src/vbd/coloring.rs:5-43

@@ -192,7 +192,7 @@ def test_step_energy_difference_matches_oracle():
     o = oracle.Solver(sc, threads=8)
     rq = min(max(st.radius + np.linalg.norm(y - x, axis=1).max(), 2 * st.radius), 4 * st.radius)
     cs = o.world.detect(o.positions(x), rq, st.ogc_c())
-    centers, radii = x, np.asarray(cs.radii)
+    centers, radii = x, np.asarray(cs["radii"])[: sc.n]
 
     def clip(p):
         d = p - centers
