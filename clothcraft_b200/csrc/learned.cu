@@ -133,7 +133,8 @@ void launch_features(const FeatureView& f, float* out, cudaStream_t st) {
     k_features<<<grid_for(f.n, 128), 128, 0, st>>>(f, out);
 }
 
-__global__ void k_learned_warm_start(FeatureView f, const float* corr, double4* alt, unsigned int* clipped) {
+__global__ void k_learned_warm_start(FeatureView f, const float* corr, double alpha, double4* alt,
+                                     unsigned int* clipped) {
     unsigned int cnt = 0;
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < f.n; v += gridDim.x * blockDim.x) {
         if (f.pinned[v]) {
@@ -141,7 +142,7 @@ __global__ void k_learned_warm_start(FeatureView f, const float* corr, double4* 
             continue;
         }
         const float* c = corr + (size_t)f.row[v] * kMlpOut;
-        d3 p = ld3(f.guess, v) + mk((double)c[0], (double)c[1], (double)c[2]) * f.unit;
+        d3 p = ld3(f.guess, v) + mk((double)c[0], (double)c[1], (double)c[2]) * (f.unit * alpha);
         if (!isfin(p)) p = ld3(f.guess, v);  // a non-finite prediction falls back per vertex
         d3 ctr = ld3(f.contacts.centers, v);
         d3 d = p - ctr;
@@ -157,10 +158,10 @@ __global__ void k_learned_warm_start(FeatureView f, const float* corr, double4* 
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(clipped, cnt);
 }
 
-void launch_learned_warm_start(const FeatureView& f, const float* corr, double4* alt, unsigned int* clipped,
-                               cudaStream_t st) {
+void launch_learned_warm_start(const FeatureView& f, const float* corr, double alpha, double4* alt,
+                               unsigned int* clipped, cudaStream_t st) {
     if (f.n == 0) return;
-    k_learned_warm_start<<<grid_for(f.n, 256), 256, 0, st>>>(f, corr, alt, clipped);
+    k_learned_warm_start<<<grid_for(f.n, 256), 256, 0, st>>>(f, corr, alpha, alt, clipped);
 }
 
 __global__ void k_targets(FeatureView f, const double4* x, float* targets) {

@@ -2,7 +2,7 @@
 // predicts the correction of the adaptive guess, and its training kernels
 // (forward, backward, Adam). No reference counterpart: the reference starts
 // every step from Prediction::guess (src/vbd/prediction.rs:15-41); the
-// learned guess replaces it only when its step energy is not higher.
+// learned guess replaces it only when its step energy is lower.
 #pragma once
 #include <cuda_fp16.h>
 
@@ -52,10 +52,10 @@ struct FeatureView {
 // out[row[v]][24] for every free vertex v.
 void launch_features(const FeatureView& f, float* out, cudaStream_t st);
 // Learned guess, clipped to the OGC ball like the warm start
-// (src/vbd.rs:316-324): alt[v] = clip(guess[v] + unit * corr[row[v]]);
+// (src/vbd.rs:316-324): alt[v] = clip(guess[v] + alpha * unit * corr[row[v]]);
 // pinned vertices copy x0. Counts clipped vertices into *clipped.
-void launch_learned_warm_start(const FeatureView& f, const float* corr, double4* alt, unsigned int* clipped,
-                               cudaStream_t st);
+void launch_learned_warm_start(const FeatureView& f, const float* corr, double alpha, double4* alt,
+                               unsigned int* clipped, cudaStream_t st);
 // targets[row[v]] = (x[v] - guess[v]) / unit for free vertices.
 void launch_targets(const FeatureView& f, const double4* x, float* targets, cudaStream_t st);
 

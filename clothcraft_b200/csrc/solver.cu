@@ -193,16 +193,24 @@ __global__ void __launch_bounds__(256) k_store_sum(const double* partial, double
     if (threadIdx.x == 0) *out = v;
 }
 
-// Keep the learned guess (already in `alt`, moving part) when its step
-// energy is not higher than the adaptive guess's (in `x`).
-__global__ void k_select_guess(uint32_t n, const double4* alt, double4* x, StepScalars* sc) {
-    bool learned = sc->e_init[1] <= sc->e_init[0];
-    if (!learned) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = alt[i];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        sc->clipped = sc->clipped_alt;
+// Scale search of the learned guess: keep the candidate if its energy is
+// lower than the best so far (the adaptive guess's to begin with).
+__global__ void k_decide_guess(StepScalars* sc) {
+    sc->take = sc->e_cand < sc->best_e ? 1 : 0;
+    if (sc->take) {
+        sc->best_e = sc->e_cand;
+        sc->clipped_best = sc->clipped_alt;
         sc->init_used = 1;
     }
+}
+__global__ void k_take_guess(uint32_t n, const double4* alt, double4* best, const StepScalars* sc) {
+    if (!sc->take) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) best[i] = alt[i];
+}
+__global__ void k_commit_guess(uint32_t n, const double4* best, double4* x, StepScalars* sc) {
+    if (!sc->init_used) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = best[i];
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->clipped = sc->clipped_best;
 }
 
 // finite result and trust-region invariant (src/vbd.rs:399-405), residual sum
@@ -363,6 +371,7 @@ struct cc_solver {
     DBuf<uint32_t> ring_off, ring, row;
     double mean_mass = 1.0;
     DBuf<float> feat, corr;
+    DBuf<double4> best;
     float* sample_features = nullptr;  // caller device buffers of cc_solver_step_sample
     float* sample_targets = nullptr;
     cudaEvent_t learn0 = nullptr, learn1 = nullptr;
@@ -551,23 +560,35 @@ void cc_solver::autotune(const SweepView& sv_in) {
     lanes = best_g;
 }
 
-// MLP correction of the adaptive guess, clipped to the OGC balls, kept only
-// when its step energy is not higher than the adaptive guess's (the adaptive
-// warm start is already in world->x()).
+// MLP correction of the adaptive guess at three scales, clipped to the OGC
+// balls; the lowest-energy candidate replaces the adaptive warm start (already
+// in world->x()) only when its step energy is lower.
 void cc_solver::learned_guess(const cc_vbd_settings& s, const cc_grab* grab, const ContactsView& cv, double rq,
                               const float* features) {
     if (!mlp) throw Failure{CC_ERR_INVALID_ARGUMENT, "learned initial guess requested but no MLP is attached"};
     FeatureView f = feature_view(cv, s, rq);
     corr.reserve((size_t)n_free * kMlpOut);
     mlp->net->forward(features, n_free, corr.ptr, mlp_precision, stream);
-    CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_alt, 0, sizeof(unsigned int), stream));
-    launch_learned_warm_start(f, corr.ptr, alt.ptr, &sc.ptr->clipped_alt, stream);
+    // Candidates guess + a u c for a in {1, 1/2, 1/4}, each clipped to the OGC
+    // balls; the one with the lowest step energy is kept if it is lower than
+    // the adaptive guess's energy, which is kept otherwise.
     SweepView sa = sweep_view(cv, s, grab);
+    best.reserve(n);
     energy_into(sa, &sc.ptr->e_init[0]);
-    sa.x = alt.ptr;
-    energy_into(sa, &sc.ptr->e_init[1]);
-    k_select_guess<<<grid_for(n, 256), 256, 0, stream>>>(n, alt.ptr, world->x(), sc.ptr);
-    own_launches += 3;
+    CC_CUDA(cudaMemcpyAsync(&sc.ptr->best_e, &sc.ptr->e_init[0], 8, cudaMemcpyDeviceToDevice, stream));
+    for (double a : {1.0, 0.5, 0.25}) {
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_alt, 0, sizeof(unsigned int), stream));
+        launch_learned_warm_start(f, corr.ptr, a, alt.ptr, &sc.ptr->clipped_alt, stream);
+        SweepView sl = sa;
+        sl.x = alt.ptr;
+        energy_into(sl, &sc.ptr->e_cand);
+        if (a == 1.0) CC_CUDA(cudaMemcpyAsync(&sc.ptr->e_init[1], &sc.ptr->e_cand, 8, cudaMemcpyDeviceToDevice, stream));
+        k_decide_guess<<<1, 1, 0, stream>>>(sc.ptr);
+        k_take_guess<<<grid_for(n, 256), 256, 0, stream>>>(n, alt.ptr, best.ptr, sc.ptr);
+        own_launches += 3;
+    }
+    k_commit_guess<<<grid_for(n, 256), 256, 0, stream>>>(n, best.ptr, world->x(), sc.ptr);
+    ++own_launches;
     CC_CUDA(cudaGetLastError());
 }
 

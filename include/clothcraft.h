@@ -99,7 +99,7 @@ typedef struct cc_ogc_settings {
 enum cc_init_mode {
     CC_INIT_ADAPTIVE = 0, /* Prediction::guess (src/vbd/prediction.rs:15-41) */
     CC_INIT_LEARNED = 1   /* MLP correction of the adaptive guess, kept only */
-                          /* when its step energy is not higher (cc_mlp_*)   */
+                          /* when its step energy is lower (cc_mlp_*)        */
 };
 /* VbdSettings (src/vbd.rs:18-52), plus two extensions without a reference
  * counterpart: the initial-guess mode and a relative-residual target.
@@ -166,8 +166,9 @@ typedef struct cc_metrics {
     double initial_relative_residual;
     int32_t has_relative_residual;
     int32_t init_used;              /* cc_init_mode the sweeps started from   */
-    double init_energy_adaptive;    /* step energy of the two initial guesses */
-    double init_energy_learned;     /* (learned mode; NaN otherwise)          */
+    double init_energy_adaptive;    /* step energy of the adaptive guess and  */
+    double init_energy_learned;     /* of the full-scale learned guess        */
+                                    /* (learned mode; NaN otherwise)          */
     double init_ms;                 /* device time of the learned guess       */
 } cc_metrics;
 
@@ -310,9 +311,10 @@ uint64_t cc_world_edges(const cc_world* world, uint32_t* edges_out);
  * vertex, a correction of the adaptive guess from 24 features of the step
  * start (inertial and previous displacement, neighbourhood, local strain,
  * nearest-contact distance). With init_mode = CC_INIT_LEARNED the solver
- * clips the learned guess to the OGC balls (ContactSet::truncate,
- * src/ogc/world.rs:91-100) and keeps it only when its step energy is not
- * higher than the adaptive guess's; cc_metrics.init_used says which one ran.
+ * forms guess + a * correction for a = 1, 1/2, 1/4, clips each to the OGC
+ * balls (ContactSet::truncate, src/ogc/world.rs:91-100) and starts from the
+ * one with the lowest step energy if that is lower than the adaptive guess's
+ * energy, else from the adaptive guess; cc_metrics.init_used says which.
  *
  * Arrays marked (device) are device pointers; the calls synchronise their
  * own stream before returning and expect the buffers to be ready. */

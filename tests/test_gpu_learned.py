@@ -1,7 +1,7 @@
 """Learned initial guess on the GPU: MLP kernels against the FP64 oracle,
-features against the oracle's restatement, the solver's learned mode and its
-energy fallback, and what a network trained on the solver's own trajectories
-gains over the adaptive guess.
+features against the oracle's restatement, the solver's learned mode with its
+energy-checked scale search and fallback, and that a guess fitted to the
+solver's own converged steps is taken and starts closer to the solution.
 
 Tolerances: FP32 inference 1e-5 relative to the output scale (FP32 sums of 64
 terms); FP16-operand tensor-core inference 1e-2 of the output scale (FP16
@@ -153,7 +153,7 @@ def test_zero_network_reproduces_the_adaptive_guess_bitwise(precision):
     net = Mlp(0)
     net.set_parameters(np.zeros(net.count, np.float32))
     for xa, xb, ma, mb in _plain_and_learned(net, precision):
-        assert mb["init_used"] == 1  # equal energies keep the learned guess
+        assert mb["init_used"] == 0  # equal energies keep the adaptive guess
         assert mb["init_energy_learned"] == mb["init_energy_adaptive"]
         assert np.array_equal(xa, xb)
 
@@ -164,9 +164,40 @@ def test_worse_guess_falls_back_to_the_adaptive_guess():
     p[-3] = 50.0  # output bias: a 50 |g| dt^2 shift in x, clipped to the OGC balls
     net.set_parameters(p)
     for xa, xb, ma, mb in _plain_and_learned(net, 1):
-        assert mb["init_used"] == 0
+        assert mb["init_used"] == 0  # no scale of the shift lowers the energy
         assert mb["init_energy_learned"] > mb["init_energy_adaptive"]
         assert np.array_equal(xa, xb)
+
+
+def test_better_guess_is_taken():
+    """A network fitted to one step's converged corrections (a sampled step)
+    must be taken on that step and must start closer to the solution."""
+    sc = contact_scene()
+    x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
+    g0 = VbdSolver(sc)
+    for _ in range(6):
+        x, v, t, _ = g0.step(x, v, t, sc.settings.to_c())
+    g = VbdSolver(sc)
+    rows = g.free_vertices
+    feat = torch.zeros((rows, 24), dtype=torch.float32, device="cuda")
+    targ = torch.zeros((rows, 3), dtype=torch.float32, device="cuda")
+    s = sc.settings
+    s.iterations, s.residual_tolerance, s.residual_check_every = 200, 1e-6, 1
+    g.set_state(x, v, t)
+    g.step_sample(s.to_c(), feat, targ)
+    net = Mlp(3)
+    net.train(feat, targ, batch=rows, steps=1500, lr=3e-3, seed=0)
+    s.residual_tolerance, s.residual_check_every = 1e-3, 1
+    runs = {}
+    for mode in (0, 1):
+        s.init_mode = mode
+        h = VbdSolver(sc)
+        h.set_mlp(net, 1)
+        _, _, _, m = h.step(x, v, t, s.to_c())
+        runs[mode] = m
+    assert runs[1]["init_used"] == 1
+    assert runs[1]["initial_relative_residual"] < runs[0]["initial_relative_residual"]
+    assert runs[1]["iterations"] <= runs[0]["iterations"]
 
 
 def test_step_energy_difference_matches_oracle():
