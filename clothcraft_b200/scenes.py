@@ -447,6 +447,138 @@ def config4(seed: int = 4, n_side: int = 1024) -> Scene:
                  StepSettings(dt=1 / 60, iterations=40, damping=1.5, radius=0.0005, stiffness=1e4), 120)
 
 
+def poisson_disk(width: float, height: float, r: float, seed: int, boundary_step: float | None = None,
+                 k: int = 30) -> tuple:
+    """Seeded Poisson-disk sample of the rectangle [0,w]x[0,h] with minimum
+    spacing r (Bridson 2007: background grid of cell r/sqrt 2, k annulus
+    candidates per active point, tested together). The perimeter is sampled
+    first at a fixed step (default r) so that two panels of the same size share
+    their edge points exactly; interior points keep a distance >= r from all
+    points. Returns (points, number of perimeter points first in the list)."""
+    rng = np.random.default_rng(seed)
+    step = r if boundary_step is None else boundary_step
+    border = []
+    for (x0, y0, x1, y1) in ((0, 0, width, 0), (width, 0, width, height), (width, height, 0, height),
+                             (0, height, 0, 0)):
+        m = max(1, int(round(math.hypot(x1 - x0, y1 - y0) / step)))
+        for i in range(m):  # corners once (start of each side)
+            t = i / m
+            border.append((x0 + t * (x1 - x0), y0 + t * (y1 - y0)))
+    border = np.asarray(border)
+    cell = r / math.sqrt(2.0)
+    gw, gh = int(math.ceil(width / cell)) + 1, int(math.ceil(height / cell)) + 1
+    grid = -np.ones((gw, gh), dtype=np.int64)
+    cap = len(border) + int(2.0 * width * height / (r * r)) + 16
+    pts = np.empty((cap, 2))
+    count = 0
+
+    def put(p):
+        nonlocal count
+        pts[count] = p
+        grid[min(int(p[0] / cell), gw - 1), min(int(p[1] / cell), gh - 1)] = count
+        count += 1
+        return count - 1
+
+    for p in border:
+        put(p)
+    nbr = int(math.ceil(3.0 * r / cell)) + 1
+    active = [put((rng.uniform(r, width - r), rng.uniform(r, height - r)))]
+    r2 = r * r
+    while active:
+        j = int(rng.integers(len(active)))
+        base = pts[active[j]]
+        ang = rng.uniform(0.0, 2.0 * math.pi, k)
+        rad = r * np.sqrt(rng.uniform(1.0, 4.0, k))
+        cand = base + np.stack([rad * np.cos(ang), rad * np.sin(ang)], axis=1)
+        ok = ((cand[:, 0] >= 0.5 * r) & (cand[:, 0] <= width - 0.5 * r) & (cand[:, 1] >= 0.5 * r) &
+              (cand[:, 1] <= height - 0.5 * r))
+        gx, gy = int(base[0] / cell), int(base[1] / cell)
+        ids = grid[max(gx - nbr, 0):gx + nbr + 1, max(gy - nbr, 0):gy + nbr + 1].ravel()
+        near = pts[ids[ids >= 0]]
+        bsel = border[(np.abs(border[:, 0] - base[0]) < 3 * r) & (np.abs(border[:, 1] - base[1]) < 3 * r)]
+        near = np.concatenate([near, bsel]) if len(bsel) else near
+        if len(near):
+            d2 = ((cand[:, None, :] - near[None, :, :]) ** 2).sum(axis=2).min(axis=1)
+            ok &= d2 >= r2
+        hit = np.nonzero(ok)[0]
+        if len(hit):
+            active.append(put(cand[hit[0]]))
+        else:
+            active[j] = active[-1]
+            active.pop()
+    return pts[:count].copy(), len(border)
+
+
+def delaunay_panel(uv: np.ndarray) -> np.ndarray:
+    """Delaunay triangles of the panel points (scipy Qhull), counter-clockwise,
+    without degenerate (area < 1e-12 of the mean) triangles."""
+    from scipy.spatial import Delaunay
+
+    tri = Delaunay(uv).simplices.astype(np.int64)
+    a, b, c = uv[tri[:, 0]], uv[tri[:, 1]], uv[tri[:, 2]]
+    cr = (b[:, 0] - a[:, 0]) * (c[:, 1] - a[:, 1]) - (b[:, 1] - a[:, 1]) * (c[:, 0] - a[:, 0])
+    tri[cr < 0] = tri[cr < 0][:, [0, 2, 1]]
+    keep = np.abs(cr) > 1e-12 * np.abs(cr).mean()
+    return tri[keep].astype(np.uint32)
+
+
+def config3(seed: int = 3, spacing: float = 0.0036) -> Scene:
+    """Sewn garment proxy: two 0.6 x 0.7 m panels (seeded Poisson-disk points,
+    ~20k each, Delaunay triangles) 5 cm either side of a fixed vertical
+    capsule (r 0.15 m, cylinder 1.2 m), joined along both side edges and the
+    outer shoulders by 1e3 N/m penalty sewing springs [(a,+1),(b,-1)] whose
+    vertex pairs are excluded from contact (src/vbd.rs:128-144). Material as
+    config 0, contact radius 1 mm, dt 1/60, 20 iterations."""
+    W, H = 0.6, 0.7
+    mat = Material.stvk_mapped()
+    panels, borders = [], []
+    for side in range(2):
+        uv, nb = poisson_disk(W, H, spacing, seed * 1009 + side, boundary_step=spacing)
+        tri = delaunay_panel(uv)
+        if side == 1:
+            tri = tri[:, [0, 2, 1]]  # back panel faces outward
+        panels.append(build_mesh(uv, tri, mat))
+        borders.append(nb)
+    mesh = concat_meshes(panels)
+    n0 = panels[0].n
+    cap_r, cap_h, gap = 0.15, 1.2, 0.05
+    y0 = 0.5 * cap_h + cap_r - H  # top edge level with the capsule's top
+    xs = []
+    for side, zsign in ((0, 1.0), (1, -1.0)):
+        uv = panels[side].uv
+        xs.append(np.stack([uv[:, 0] - 0.5 * W, y0 + uv[:, 1], np.full(len(uv), zsign * (cap_r + gap))], axis=1))
+    x = np.ascontiguousarray(np.concatenate(xs))
+    # seams: perimeter points are identical on both panels (same order, same uv)
+    ub = panels[0].uv[:borders[0]]
+    assert np.array_equal(ub, panels[1].uv[:borders[1]])
+    side_seam = (np.abs(ub[:, 0]) < 1e-12) | (np.abs(ub[:, 0] - W) < 1e-12)
+    shoulder = (np.abs(ub[:, 1] - H) < 1e-12) & ((ub[:, 0] <= 0.2 + 1e-12) | (ub[:, 0] >= W - 0.2 - 1e-12))
+    ids = np.nonzero(side_seam | shoulder)[0]
+    mesh.stitch_offsets = np.arange(0, 2 * len(ids) + 1, 2, dtype=np.uint32)
+    mesh.stitch_vertices = np.stack([ids, ids + n0], axis=1).ravel().astype(np.uint32)
+    mesh.stitch_weights = np.tile([1.0, -1.0], len(ids))
+    mesh.stitch_stiffness = np.full(len(ids), 1e3)
+    return Scene("garment_capsule", mesh, capsule(cap_r, cap_h), x, np.zeros_like(x),
+                 StepSettings(dt=1 / 60, iterations=20, damping=1.5, radius=0.001, stiffness=1e4), 120,
+                 note="seed=%d, %d stitches" % (seed, len(ids)))
+
+
+def driven_corners(sc: Scene, x: np.ndarray, time: float, speed: float = 0.2) -> np.ndarray:
+    """Config-4 kinematics: the pinned corners move toward the sheet's centre
+    at `speed` m/s; returns x with the pinned rows set for `time`. The caller
+    edits the pinned positions between steps (the reference has no driven
+    pins; this invalidates the adaptive-guess history every step)."""
+    pins = np.nonzero(sc.mesh.pinned)[0]
+    start = sc.mesh.pin_positions[pins]
+    centre = sc.x0.mean(axis=0)
+    d = centre - start
+    d[:, 1] = 0.0
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    out = x.copy()
+    out[pins] = start + d * (speed * time)
+    return out
+
+
 def small_sheet(n_side: int = 16, seed: int = 0, obstacle: bool = True, iterations: int = 20,
                 radius: float = 0.002, height: float = 0.3, side: float = 0.5, pins=None) -> Scene:
     """Reduced config-0 style scene for fast parity tests."""
