@@ -1,15 +1,22 @@
 #!/usr/bin/env python
-"""Benchmark: VBD+OGC steps/s on the 256x256 self-contact fold.
+"""Benchmark: VBD+OGC steps/s at equal residual on the 256x256 self-contact fold.
 
-Workload (one "step" = one implicit-Euler VBD step with on-GPU OGC
-detection, colouring and 30 colour sweeps): a 256x256-vertex sheet (65,536
-vertices, 130,050 triangles), 1 m side, dropped from y=0.5 m with a seeded
-tilt onto a fixed r=0.3 m sphere so that it folds onto itself; OGC radius
-1 mm, contact stiffness 1e4 N/m, dt 1/60 s, 30 iterations. Synthetic, seeded.
-Timing starts in the fold phase: both arms load the scene's state after
-PHASE_START steps (t = 3.33 s, ~95k retained contact terms; committed as
-tests/golden/sheet256_fold_state.npz with its generator), then run W warm-up
-steps and K timed steps.
+Workload (one "step" = one implicit-Euler VBD step with on-GPU OGC detection,
+colouring and colour sweeps): a 256x256-vertex sheet (65,536 vertices,
+130,050 triangles), 1 m side, dropped from y=0.5 m with a seeded tilt onto a
+fixed r=0.3 m sphere so that it folds onto itself; OGC radius 1 mm, contact
+stiffness 1e4 N/m, dt 1/60 s. Synthetic, seeded. Timing starts in the fold
+phase: every arm loads the scene's state after PHASE_START steps (t = 3.33 s,
+~95k retained contact terms; tests/golden/sheet256_fold_state.npz with its
+generator), then runs W warm-up and K timed steps.
+
+Equal residual: every step iterates until the relative force residual
+||P grad E(x)|| / ||grad E(y)|| <= 1e-3 (evaluated every 2 iterations, at most
+200 iterations, the reference's limit). `value` is the learned-init form
+(MLP correction of the adaptive guess, energy-checked); the plain adaptive
+init runs alongside (`plain`), and so does the reference's fixed 30-iteration
+step (`fixed_iterations`). The network is clothcraft_b200/data/fold_init_mlp.npz,
+trained by `python -m clothcraft_b200.train_init fold` on other seeds.
 
   python bench.py [--gpus N --steps K --warmup W]      # B200 library
   python bench.py --impl reference [...]                # CPU path (oracle restatement)
@@ -33,7 +40,13 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-METRIC = "VBD steps/s (256x256 self-contact fold, 30 iterations, 1 GPU replica)"
+METRIC = ("VBD steps/s at equal residual (relative force residual <= 1e-3), learned init vs plain, "
+          "256x256 self-contact fold, 1 GPU")
+TOLERANCE = 1e-3
+CHECK_EVERY = 2
+ITERATION_CAP = 200
+FIXED_ITERATIONS = 30
+MLP_PATH = os.path.join(ROOT, "clothcraft_b200", "data", "fold_init_mlp.npz")
 UNIT = "steps/s"
 L2_FLUSH_BYTES = 256 << 20
 PHASE_START = 200
@@ -79,10 +92,13 @@ def config_dict(sc, n_gpus):
     return {
         "workload": "sheet256_fold: 256x256 sheet (65,536 v / 130,050 t), 1 m, seeded tilt, dropped onto a "
                     "fixed r=0.3 m icosphere (2,562 v), OGC VF+EE self-contact r=1 mm, k=1e4 N/m, "
-                    "dt=1/60 s, 30 VBD iterations, StVK-mapped membrane (mu=1e4, lambda=2e4 N/m)",
+                    "dt=1/60 s, StVK-mapped membrane (mu=1e4, lambda=2e4 N/m); iterations until the "
+                    "relative force residual <= 1e-3 (checked every 2, cap 200)",
         "vertices": int(sc.n),
         "triangles": int(len(sc.mesh.triangles)),
-        "iterations": int(sc.settings.iterations),
+        "residual_tolerance": TOLERANCE,
+        "residual_check_every": CHECK_EVERY,
+        "iteration_cap": ITERATION_CAP,
         "l2": "flushed between timed steps (256 MiB device write outside the timed events)",
         "phase": "timed steps start at step %d + warm-up (fold phase, contact-rich)" % PHASE_START,
         "parallelism": "replicas x%d (single cloth does not shard)" % n_gpus,
@@ -170,49 +186,56 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_run(sc, state, steps, budget_s, threads):
-    """The reference CPU path (FP64 oracle restatement, all host threads) on
-    the same workload from `state`; stops after `steps` or `budget_s`."""
+def step_settings(sc, mode, iterations=None):
+    """Equal-residual settings (mode 0 adaptive, 1 learned), or a fixed
+    iteration count with no residual target when `iterations` is given."""
+    s = sc.settings
+    if iterations is None:
+        s.iterations, s.residual_tolerance, s.residual_check_every = ITERATION_CAP, TOLERANCE, CHECK_EVERY
+    else:
+        s.iterations, s.residual_tolerance, s.residual_check_every = iterations, 0.0, 0
+    s.init_mode = mode
+    return s.to_c()
+
+
+def cpu_reference_run(sc, state, steps, budget_s, threads, warmup=0):
+    """The reference CPU path (FP64 oracle restatement, all host threads) at
+    equal residual on the same workload from `state`: `warmup` untimed steps,
+    then up to `steps` timed steps or `budget_s`. Returns (done, seconds,
+    iterations of the timed steps, warm-up steps run)."""
     import oracle
 
     o = oracle.Solver(sc, threads=threads)
-    st = sc.settings.to_c()
+    st = step_settings(sc, 0)
     x, v, t = state
-    done = 0
     t0 = time.perf_counter()
-    while done < steps:
+    warm = 0
+    for _ in range(warmup):
+        if time.perf_counter() - t0 > budget_s / 2:
+            break
         x, v, t, _ = o.step(x, v, t, st)
+        warm += 1
+    done, its = 0, []
+    t1 = time.perf_counter()
+    while done < steps:
+        x, v, t, m = o.step(x, v, t, st)
+        its.append(int(m["iterations"]))
         done += 1
         if time.perf_counter() - t0 > budget_s:
             break
-    dt = time.perf_counter() - t0
-    return done, dt
+    return done, time.perf_counter() - t1, its, warm
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    from clothcraft_b200 import scenes  # noqa: F401
-
     sc = workload()
     threads = os.cpu_count() or 1
-    st = sc.settings.to_c()
-    import oracle
-
-    o = oracle.Solver(sc, threads=threads)
-    x, v, t = fold_state()
     budget = float(os.environ.get("CC_REFERENCE_BUDGET_S", "150"))
-    t0 = time.perf_counter()
-    warm = 0
-    for _ in range(args.warmup):
-        if time.perf_counter() - t0 > budget / 2:
-            break
-        x, v, t, _ = o.step(x, v, t, st)
-        warm += 1
-    done, dt = cpu_reference_run(sc, (x, v, t), args.steps, budget - (time.perf_counter() - t0), threads)
+    done, dt, its, warm = cpu_reference_run(sc, fold_state(), args.steps, budget, threads, warmup=args.warmup)
     value = done / dt
-    sample = "%d warm-up + %d timed steps from the fold-phase state (bounded to ~%.0f s), %d host threads" % (
-        warm, done, budget, threads)
+    sample = ("%d warm-up + %d timed steps from the fold-phase state at equal residual (bounded to ~%.0f s), "
+              "%d host threads, iterations %s" % (warm, done, budget, threads, its))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done, "warmup": warm,
         "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
@@ -220,8 +243,10 @@ def run_reference(args, rank, world):
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "C++ FP64 restatement of the reference CPU path (VbdSolver::step + OgcWorld::detect); the Rust "
-                "original cannot be compiled in this environment",
+        "mean_iterations": float(np.mean(its)) if its else None,
+        "note": "C++ FP64 restatement of the reference CPU path (VbdSolver::step + OgcWorld::detect, adaptive "
+                "init) run to the same residual target; the Rust original cannot be compiled in this "
+                "environment",
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -230,7 +255,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -260,26 +285,32 @@ def main():
         torch.cuda.set_device(0)
 
     from clothcraft_b200 import native
+    from clothcraft_b200.learned import Mlp
     from clothcraft_b200.vbd import VbdSolver
 
+    if not os.path.exists(MLP_PATH):
+        raise SystemExit("missing %s: train it with `python -m clothcraft_b200.train_init fold`" % MLP_PATH)
     L = native.load()
     L.cc_set_device(local if world > 1 else 0)
     sc = workload()
-    st = sc.settings.to_c()
-    solver = VbdSolver(sc)
-    if args.lanes:
-        if L.cc_solver_set_lanes(solver.h, args.lanes) != 0:
-            raise SystemExit("invalid --lanes %d" % args.lanes)
-    stream = torch.cuda.ExternalStream(L.cc_solver_stream(solver.h))
+    net = Mlp.load(MLP_PATH)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-    solver.set_state(*fold_state())
-    for _ in range(args.warmup):
-        solver.step_resident(st)
-    warm_state = solver.get_state()
+    start = fold_state()
 
-    def timed(step_fn, k):
-        evs = []
-        metrics = []
+    def make(mode, iterations=None):
+        s = VbdSolver(sc)
+        if args.lanes and L.cc_solver_set_lanes(s.h, args.lanes) != 0:
+            raise SystemExit("invalid --lanes %d" % args.lanes)
+        if mode:
+            s.set_mlp(net, 1)
+        s.set_state(*start)
+        for _ in range(args.warmup):
+            s.step_resident(step_settings(sc, mode, iterations))
+        return s
+
+    def timed(solver, step_fn, k):
+        stream = torch.cuda.ExternalStream(L.cc_solver_stream(solver.h))
+        evs, metrics = [], []
         for _ in range(k):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -293,69 +324,83 @@ def main():
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs), metrics
 
-    # ---- device-resident throughput (value); clocks sampled over all GPU legs
-    clocks = ClockSampler(local).__enter__()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms, mets = timed(lambda: solver.step_resident(st), args.steps)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t_max = ms
-    if dist:
+    def max_over_ranks(ms):
+        if not dist:
+            return ms
         tt = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * args.steps / (t_max / 1000.0)
+        return float(tt.item())
 
-    # ---- end to end through the C ABI with host buffers (e2e)
-    x, v, t = warm_state
-    n = sc.n
-    state = {"x": x.copy(), "v": v.copy(), "t": t}
+    def leg(solver, step_fn, k):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms, mets = timed(solver, step_fn, k)
+        if dist:
+            dist.barrier()
+        return max_over_ranks(ms), mets
+
+    K = args.steps
+    st_l, st_p = step_settings(sc, 1), step_settings(sc, 0)
+    learned, plain = make(1), make(0)
+    warm_learned = learned.get_state()
+    clocks = ClockSampler(local).__enter__()
+    # ---- value: learned init at equal residual, device-resident
+    t_l, mets_l = leg(learned, lambda: learned.step_resident(st_l), K)
+    # ---- plain adaptive init at equal residual
+    t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
+    # ---- end to end through cc_solver_step with host arrays (learned)
+    e2e_solver = make(1)
+    x, v, t = e2e_solver.get_state()
+    state = {"x": x, "v": v, "t": t}
 
     def host_step():
-        state["x"], state["v"], state["t"], m = solver.step(state["x"], state["v"], state["t"], st)
+        state["x"], state["v"], state["t"], m = e2e_solver.step(state["x"], state["v"], state["t"], st_l)
         return m
 
-    host_step()  # warm the host path once
-    if dist:
-        dist.barrier()
-    ms_e2e, _ = timed(host_step, args.steps)
-    e2e_max = ms_e2e
-    if dist:
-        tt = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_max = float(tt.item())
-    e2e_value = world * args.steps / (e2e_max / 1000.0)
-
-    # ---- per-launch sweep timing (events around every sweep launch), same
-    # state and step count as the value leg, for the roofline
-    solver.set_state(*warm_state)
-    L.cc_solver_set_profiling(solver.h, 1)
-    _, mets = timed(lambda: solver.step_resident(st), args.steps)
-    L.cc_solver_set_profiling(solver.h, 0)
+    t_e2e, _ = leg(e2e_solver, host_step, K)
+    # ---- per-launch sweep timing for the roofline (learned, same start)
+    learned.set_state(*warm_learned)
+    L.cc_solver_set_profiling(learned.h, 1)
+    _, mets_prof = leg(learned, lambda: learned.step_resident(st_l), K)
+    L.cc_solver_set_profiling(learned.h, 0)
+    # ---- the reference's fixed-iteration step (plain init, 30 iterations), for context
+    st_f = step_settings(sc, 0, FIXED_ITERATIONS)
+    st_f.residual_check_every = FIXED_ITERATIONS  # one residual evaluation, after the last iteration
+    fixed = make(0, FIXED_ITERATIONS)
+    t_f, mets_f = leg(fixed, lambda: fixed.step_resident(st_f), K)
     clocks.__exit__(None, None, None)
 
-    # ---- roofline of the dominant kernel (colour sweep)
+    value = world * K / (t_l / 1000.0)
+    free = int((sc.mesh.pinned == 0).sum())
+
+    def iters(mets):
+        return [int(m["iterations"]) for m in mets]
+
+    def summary(t_ms, mets):
+        its = iters(mets)
+        return {"steps_per_s": world * K / (t_ms / 1000.0), "ms_per_step": t_ms / K,
+                "vertex_iters_per_s": world * free * sum(its) / (t_ms / 1000.0),
+                "mean_iterations": float(np.mean(its)), "median_iterations": float(np.median(its)),
+                "capped_fraction": float(np.mean(np.array(its) >= ITERATION_CAP)),
+                "mean_final_relative_residual": float(np.mean([m["relative_residual"] for m in mets]))}
+
+    # ---- roofline of the dominant kernel (colour sweep), learned leg
     peak, peak_kind = load_peaks()
     static_b = static_bytes_per_sweep(sc)
-    sweep_ms = sum(m["sweep_ms"] for m in mets)
-    sweeps = sum(m["sweep_launches"] for m in mets)
-    iters = sum(m["iterations"] for m in mets)
-    alg_bytes = sum(static_b * m["iterations"] + 28.0 * m["contact_incidence"] * m["iterations"] for m in mets)
+    sweep_ms = sum(m["sweep_ms"] for m in mets_prof)
+    sweeps = sum(m["sweep_launches"] for m in mets_prof)
+    alg_bytes = sum((static_b + 28.0 * m["contact_incidence"]) * m["iterations"] for m in mets_prof)
     achieved = alg_bytes / (sweep_ms / 1000.0) / 1e9 if sweep_ms > 0 else None
-    free = int((sc.mesh.pinned == 0).sum())
-    launches = int(sum(m["kernel_launches"] for m in mets))
 
-    # ---- CPU baseline (rank 0, N=1 only)
+    # ---- CPU baseline (rank 0, N=1 only): the oracle at equal residual
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        done, dt = cpu_reference_run(sc, warm_state, 2, 25.0, threads)
+        done, dt, its_cpu, _ = cpu_reference_run(sc, start, 3, 25.0, threads)
         cpu = {"value": done / dt, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": "%d step(s) of the same workload from the post-warm-up state, FP64 oracle restatement of "
-                         "the reference CPU path, %d threads" % (done, threads)}
+               "sample": "first %d step(s) from the fold-phase state at equal residual (iterations %s), FP64 "
+                         "oracle restatement of the reference CPU path, %d threads" % (done, its_cpu, threads)}
 
     if dist:
         dist.barrier()
@@ -367,16 +412,24 @@ def main():
         "value": value,
         "unit": UNIT,
         "n_gpus": world,
-        "steps": args.steps,
+        "steps": K,
         "warmup": args.warmup,
-        "ms_per_step": t_max / args.steps,
+        "ms_per_step": t_l / K,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
         "config": config_dict(sc, world),
-        "vertex_iters_per_s": world * free * iters / (t_max / 1000.0),
+        "learned": summary(t_l, mets_l),
+        "plain": summary(t_p, mets_p),
+        "learned_vs_plain_time_ratio": t_p / t_l,
+        "learned_init_used_fraction": float(np.mean([m["init_used"] for m in mets_l])),
+        "fixed_iterations": {"iterations": FIXED_ITERATIONS, "steps_per_s": world * K / (t_f / 1000.0),
+                             "ms_per_step": t_f / K,
+                             "mean_final_relative_residual": float(np.mean([m["relative_residual"]
+                                                                            for m in mets_f]))},
+        "vertex_iters_per_s": world * free * sum(iters(mets_l)) / (t_l / 1000.0),
         "roofline": {
             "kernel": "k_sweep (colour sweep)",
             "bound": "hbm",
@@ -390,22 +443,23 @@ def main():
             "peak_kind": peak_kind,
             "sweep_launches": int(sweeps),
             "avg_launch_us": 1000.0 * sweep_ms / max(sweeps, 1),
-            "algorithmic_bytes_per_step": alg_bytes / args.steps,
             "algorithmic_bytes_per_launch": alg_bytes / max(sweeps, 1),
-            "sweep_share_of_step": sweep_ms / ms if ms > 0 else None,
+            "sweep_share_of_step": sweep_ms / max(sum(m["gpu_compute_ms"] for m in mets_prof), 1e-9),
         },
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 32, "d2h_bytes_per_step": 2 * n * 32},
-        "gpu_launches": launches,
-        "lanes_per_vertex": int(L.cc_solver_get_lanes(solver.h)),
+        "e2e": {"value": world * K / (t_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 2 * sc.n * 32,
+                "d2h_bytes_per_step": 2 * sc.n * 32},
+        "gpu_launches": int(sum(m["kernel_launches"] for m in mets_l)),
+        "lanes_per_vertex": int(L.cc_solver_get_lanes(learned.h)),
         "breakdown_ms_per_step": {
-            "detection": sum(m["detection_ms"] for m in mets) / args.steps,
-            "coloring": sum(m["color_ms"] for m in mets) / args.steps,
-            "sweeps": sweep_ms / args.steps,
+            "detection": sum(m["detection_ms"] for m in mets_l) / K,
+            "coloring": sum(m["color_ms"] for m in mets_l) / K,
+            "learned_guess": sum(m["init_ms"] for m in mets_l) / K,
+            "sweeps": sweep_ms / K,
         },
         "clocks": clocks.summary(),
-        "detections_per_step": sum(m["detection_updates"] for m in mets) / args.steps,
-        "contact_terms_last": mets[-1]["contact_terms"] if mets else None,
+        "detections_per_step": sum(m["detection_updates"] for m in mets_l) / K,
+        "contact_terms_last": mets_l[-1]["contact_terms"] if mets_l else None,
     }
     print(json.dumps(line), flush=True)
     return 0
