@@ -369,6 +369,14 @@ def main():
     st_f.residual_check_every = FIXED_ITERATIONS  # one residual evaluation, after the last iteration
     fixed = make(0, FIXED_ITERATIONS)
     t_f, mets_f = leg(fixed, lambda: fixed.step_resident(st_f), K)
+    # ---- the reference's iteration budget (30) with the same residual target:
+    # steps stop early once converged; both inits
+    budget = {}
+    for mode in (0, 1):
+        sb = step_settings(sc, mode)
+        sb.iterations = FIXED_ITERATIONS
+        solver_b = make(mode, FIXED_ITERATIONS)
+        budget[mode] = leg(solver_b, lambda: solver_b.step_resident(sb), K)
     clocks.__exit__(None, None, None)
 
     value = world * K / (t_l / 1000.0)
@@ -429,6 +437,8 @@ def main():
                              "ms_per_step": t_f / K,
                              "mean_final_relative_residual": float(np.mean([m["relative_residual"]
                                                                             for m in mets_f]))},
+        "budget_30_iterations": {"learned": summary(*budget[1]), "plain": summary(*budget[0]),
+                                 "note": "same residual target, at most 30 iterations (the reference's count)"},
         "vertex_iters_per_s": world * free * sum(iters(mets_l)) / (t_l / 1000.0),
         "roofline": {
             "kernel": "k_sweep (colour sweep)",
