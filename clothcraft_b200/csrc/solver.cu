@@ -376,6 +376,8 @@ struct cc_solver {
     float* sample_targets = nullptr;
     cudaEvent_t learn0 = nullptr, learn1 = nullptr;
     bool learn_timed = false;
+    // batched instances (cc_batch_create): first vertex and count of each
+    std::vector<uint64_t> inst_first, inst_count;
     std::string err;
     int code = 0;
     int fail(const Failure& f) {
@@ -1560,6 +1562,117 @@ int32_t cc_solver_step_sample(cc_solver* s, const cc_vbd_settings* settings, con
     } catch (const Failure& f) {
         return s->fail(f);
     }
+}
+
+// ------------------------------------------------------ batched instances
+// Many independent cloths as one solver: meshes concatenated (vertex, triangle,
+// hinge, stitch and material indices offset), obstacles concatenated. Each
+// colour sweep then covers every instance in one launch, detection builds
+// one hierarchy for all of them, and the colouring of the union equals each
+// instance's own greedy colouring (instances share no edges). Contact between
+// instances is the caller's to avoid by placement: detection finds any pair
+// within the query radius, whichever instances it joins.
+int32_t cc_batch_create(const cc_mesh* meshes, const cc_surface* obstacles, const double* const* x0,
+                        const double* const* v0, uint64_t count, cc_solver** out) {
+    try {
+        if (!meshes || !x0 || !out || count == 0) throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_batch_create: bad arguments"};
+        std::vector<uint32_t> tri, tmat, hin, hmat, soff{0}, sv;
+        std::vector<double> inv, area, hw, hac, masses, ppos, sw, sk, xs, vs;
+        std::vector<uint8_t> pin;
+        std::vector<cc_material> mats;
+        std::vector<double> ov;
+        std::vector<uint32_t> ot;
+        std::vector<uint64_t> first, cnt;
+        uint64_t nv = 0, obase = 0;
+        for (uint64_t k = 0; k < count; ++k) {
+            const cc_mesh& m = meshes[k];
+            if (!x0[k]) throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_batch_create: missing positions"};
+            uint32_t mbase = (uint32_t)mats.size(), vb = (uint32_t)nv;
+            first.push_back(nv);
+            cnt.push_back(m.n_vertices);
+            for (uint64_t i = 0; i < m.n_materials; ++i) mats.push_back(m.materials[i]);
+            for (uint64_t t = 0; t < m.n_triangles; ++t) {
+                for (int c = 0; c < 3; ++c) tri.push_back(m.triangles[3 * t + c] + vb);
+                for (int c = 0; c < 4; ++c) inv.push_back(m.inv_dm[4 * t + c]);
+                area.push_back(m.area[t]);
+                tmat.push_back((m.triangle_material ? m.triangle_material[t] : 0) + mbase);
+            }
+            for (uint64_t h = 0; h < m.n_hinges; ++h) {
+                for (int c = 0; c < 4; ++c) hin.push_back(m.hinges[4 * h + c] + vb);
+                hw.push_back(m.hinge_weight[h]);
+                hac.push_back(m.hinge_across[2 * h]);
+                hac.push_back(m.hinge_across[2 * h + 1]);
+                hmat.push_back((m.hinge_material ? m.hinge_material[h] : 0) + mbase);
+            }
+            for (uint64_t i = 0; i < m.n_vertices; ++i) {
+                masses.push_back(m.masses[i]);
+                pin.push_back(m.pinned ? m.pinned[i] : 0);
+                for (int c = 0; c < 3; ++c) {
+                    ppos.push_back(m.pin_positions ? m.pin_positions[3 * i + c] : 0.0);
+                    xs.push_back(x0[k][3 * i + c]);
+                    vs.push_back(v0 && v0[k] ? v0[k][3 * i + c] : 0.0);
+                }
+            }
+            for (uint64_t st = 0; st < m.n_stitches; ++st) {
+                for (uint32_t a = m.stitch_offsets[st]; a < m.stitch_offsets[st + 1]; ++a) {
+                    sv.push_back(m.stitch_vertices[a] + vb);
+                    sw.push_back(m.stitch_weights[a]);
+                }
+                soff.push_back((uint32_t)sv.size());
+                sk.push_back(m.stitch_stiffness[st]);
+            }
+            if (obstacles && obstacles[k].n_vertices) {
+                const cc_surface& o = obstacles[k];
+                for (uint64_t i = 0; i < 3 * o.n_vertices; ++i) ov.push_back(o.vertices[i]);
+                for (uint64_t t = 0; t < 3 * o.n_triangles; ++t) {
+                    if (o.triangles[t] >= o.n_vertices) throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid avatar index"};
+                    ot.push_back(o.triangles[t] + (uint32_t)obase);
+                }
+                obase += o.n_vertices;
+            }
+            nv += m.n_vertices;
+        }
+        if (nv > 0x0fffffffull) throw Failure{CC_ERR_INVALID_ARGUMENT, "cc_batch_create: too many vertices"};
+        cc_mesh u{};
+        u.n_vertices = nv;
+        u.n_triangles = area.size();
+        u.triangles = tri.data();
+        u.inv_dm = inv.data();
+        u.area = area.data();
+        u.triangle_material = tmat.data();
+        u.n_hinges = hw.size();
+        u.hinges = hin.data();
+        u.hinge_weight = hw.data();
+        u.hinge_across = hac.data();
+        u.hinge_material = hmat.data();
+        u.n_materials = mats.size();
+        u.materials = mats.data();
+        u.masses = masses.data();
+        u.pinned = pin.data();
+        u.pin_positions = ppos.data();
+        u.n_stitches = sk.size();
+        u.stitch_offsets = soff.data();
+        u.stitch_vertices = sv.data();
+        u.stitch_weights = sw.data();
+        u.stitch_stiffness = sk.data();
+        cc_surface os{obase, ov.data(), ot.size() / 3, ot.data()};
+        int32_t rc = cc_solver_create(&u, obase ? &os : nullptr, xs.data(), vs.data(), nv, out);
+        if (rc != CC_OK) return rc;
+        (*out)->inst_first = first;
+        (*out)->inst_count = cnt;
+        return CC_OK;
+    } catch (const Failure& f) {
+        return set_global(f.code, f.message);
+    }
+}
+
+uint64_t cc_batch_instances(const cc_solver* s, uint64_t* first_vertex, uint64_t* vertex_count, uint64_t capacity) {
+    uint64_t k = s->inst_first.size();
+    for (uint64_t i = 0; i < k && i < capacity; ++i) {
+        if (first_vertex) first_vertex[i] = s->inst_first[i];
+        if (vertex_count) vertex_count[i] = s->inst_count[i];
+    }
+    return k;
 }
 
 }  // extern "C"

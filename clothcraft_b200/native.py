@@ -51,6 +51,9 @@ SIGNATURES = {
                                     C.POINTER(cc_contacts)]),
     "cc_world_candidates": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_candidates)]),
     "cc_world_edges": (C.c_uint64, [C.c_void_p, c_uint32_p]),
+    "cc_batch_create": (C.c_int32, [C.POINTER(cc_mesh), C.POINTER(cc_surface), C.POINTER(c_double_p),
+                                    C.POINTER(c_double_p), C.c_uint64, C.POINTER(C.c_void_p)]),
+    "cc_batch_instances": (C.c_uint64, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_uint64]),
     "cc_mlp_create": (C.c_int32, [C.c_uint64, C.POINTER(C.c_void_p)]),
     "cc_mlp_destroy": (None, [C.c_void_p]),
     "cc_mlp_last_error": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_uint64]),

@@ -563,6 +563,77 @@ def config3(seed: int = 3, spacing: float = 0.0036) -> Scene:
                  note="seed=%d, %d stitches" % (seed, len(ids)))
 
 
+def config2_instances(seed: int = 2, count: int = 96, sides=(32, 320), pitch: float = 3.0) -> list:
+    """Batched uneven instances: `count` square sheets whose vertex side is
+    drawn from U{sides} (1k-102k vertices each, ~3.6M in total for 96), at the
+    config-0 vertex spacing (0.5 m / 63 cells), 1-4 random corners pinned,
+    moduli x U(0.5, 2) of config 0's, each with its own icosphere below it
+    (r = 0.2 side, sheet 0.6 side above its centre). Instances sit on a
+    10-wide grid `pitch` m apart, so no two come within contact range.
+    Contact radius 2 mm, stiffness 1e4 N/m, dt 1/60 s, 20 iterations."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.integers(sides[0], sides[1] + 1))
+        side = (n - 1) * (0.5 / 63)
+        scale = float(rng.uniform(0.5, 2.0))
+        mat = Material.stvk_mapped(mu=1.0e4 * scale, lam=2.0e4 * scale)
+        corners = np.array([0, n - 1, n * (n - 1), n * n - 1])
+        pins = tuple(int(c) for c in np.sort(rng.choice(corners, int(rng.integers(1, 5)), replace=False)))
+        mesh, x = sheet(n, side, 0.6 * side, mat, jitter=1e-4, seed=seed * 100003 + k, pins=pins)
+        off = np.array([(k % 10) * pitch, 0.0, (k // 10) * pitch])
+        x = np.ascontiguousarray(x + off)
+        mesh.pin_positions[list(pins)] += off
+        obs = icosphere(3, 0.2 * side, center=tuple(off))
+        out.append(Scene("batch%d_sheet%d" % (k, n), mesh, obs, x, np.zeros_like(x),
+                         StepSettings(dt=1 / 60, iterations=20, damping=1.5, radius=0.002, stiffness=1e4), 120,
+                         note="side %d, pins %s, moduli x%.3f" % (n, pins, scale)))
+    return out
+
+
+def batch_scene(instances: list) -> Scene:
+    """The union of instances as one scene (vertex order = instance order,
+    obstacles concatenated), the layout cc_batch_create builds."""
+    mesh = concat_meshes([sc.mesh for sc in instances])
+    so, sv, sw, sk = [np.zeros(1, np.uint32)], [], [], []
+    off, base = 0, 0
+    for sc in instances:
+        m = sc.mesh
+        so.append(m.stitch_offsets[1:].astype(np.int64) + base)
+        sv.append(m.stitch_vertices.astype(np.int64) + off)
+        sw.append(m.stitch_weights)
+        sk.append(m.stitch_stiffness)
+        base += len(m.stitch_vertices)
+        off += m.n
+    mesh.stitch_offsets = np.concatenate(so).astype(np.uint32)
+    mesh.stitch_vertices = np.concatenate(sv).astype(np.uint32)
+    mesh.stitch_weights = np.concatenate(sw).astype(np.float64)
+    mesh.stitch_stiffness = np.concatenate(sk).astype(np.float64)
+    verts, faces, ob = [], [], 0
+    for sc in instances:
+        if sc.obstacle is not None:
+            verts.append(sc.obstacle.vertices)
+            faces.append(sc.obstacle.triangles.astype(np.int64) + ob)
+            ob += len(sc.obstacle.vertices)
+    obs = Obstacle(np.concatenate(verts), np.concatenate(faces).astype(np.uint32)) if verts else None
+    x = np.ascontiguousarray(np.concatenate([sc.x0 for sc in instances]))
+    v = np.ascontiguousarray(np.concatenate([sc.v0 for sc in instances]))
+    return Scene("batch%d" % len(instances), mesh, obs, x, v, instances[0].settings, instances[0].steps,
+                 note="%d instances, %d vertices" % (len(instances), len(x)))
+
+
+def partition_instances(sizes, parts: int) -> list:
+    """Greedy longest-first bin packing of instances (by vertex count) onto
+    `parts` GPUs: returns, per part, the ascending instance indices."""
+    loads = [0] * parts
+    bins = [[] for _ in range(parts)]
+    for i in sorted(range(len(sizes)), key=lambda i: (-sizes[i], i)):
+        p = min(range(parts), key=lambda q: (loads[q], q))
+        bins[p].append(i)
+        loads[p] += sizes[i]
+    return [sorted(b) for b in bins]
+
+
 def driven_corners(sc: Scene, x: np.ndarray, time: float, speed: float = 0.2) -> np.ndarray:
     """Config-4 kinematics: the pinned corners move toward the sheet's centre
     at `speed` m/s; returns x with the pinned rows set for `time`. The caller

@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import abi, native
-from .abi import cc_candidates, cc_grab, cc_metrics, cc_surface
+from .abi import cc_candidates, cc_grab, cc_mesh, cc_metrics, cc_surface
 
 
 class VbdError(RuntimeError):
@@ -157,6 +157,52 @@ class VbdSolver:
         self.total = int(L.cc_solver_total(h))
         self.obstacle_x = None if scene.obstacle is None else abi.as_f64(scene.obstacle.vertices)
         self.world = OgcWorld(None, None, self.n, _handle=L.cc_solver_world(h), _owner=self)
+
+    @classmethod
+    def batch(cls, instances):
+        """Many independent scenes stepped as one solver (cc_batch_create);
+        state arrays hold the instances' vertices in order."""
+        L = native.load()
+        keep = []
+        k = len(instances)
+        meshes = (cc_mesh * k)()
+        obst = (cc_surface * k)()
+        xs = (abi.c_double_p * k)()
+        vs = (abi.c_double_p * k)()
+        for i, sc in enumerate(instances):
+            m, km = sc.mesh.to_c()
+            meshes[i] = m
+            keep.append(km)
+            if sc.obstacle is not None:
+                o, ko = sc.obstacle.to_c()
+                obst[i] = o
+                keep.append(ko)
+            x = abi.as_f64(sc.x0)
+            v = abi.as_f64(sc.v0)
+            keep += [x, v]
+            xs[i] = _f64p(x)
+            vs[i] = _f64p(v)
+        h = C.c_void_p()
+        rc = L.cc_batch_create(meshes, obst, xs, vs, k, C.byref(h))
+        if rc != 0:
+            raise _global_error(rc)
+        self = cls.__new__(cls)
+        self.h = h
+        self.n = int(L.cc_solver_moving(h))
+        self.total = int(L.cc_solver_total(h))
+        obs = [sc.obstacle.vertices for sc in instances if sc.obstacle is not None]
+        self.obstacle_x = abi.as_f64(np.concatenate(obs)) if obs else None
+        self.world = OgcWorld(None, None, self.n, _handle=L.cc_solver_world(h), _owner=self)
+        return self
+
+    def instances(self):
+        """(first vertex, vertex count) of each batched instance."""
+        L = native.load()
+        k = int(L.cc_batch_instances(self.h, None, None, 0))
+        f = (C.c_uint64 * max(k, 1))()
+        c = (C.c_uint64 * max(k, 1))()
+        L.cc_batch_instances(self.h, f, c, k)
+        return [(int(f[i]), int(c[i])) for i in range(k)]
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -306,6 +306,25 @@ int32_t cc_world_candidates(cc_world* world, const double* x, double radius,
 /* Topology sizes: edges of the combined mesh (src/ogc/topology.rs:13-52). */
 uint64_t cc_world_edges(const cc_world* world, uint32_t* edges_out);
 
+/* -------------------------------------------------- batched instances */
+/* Many independent cloths stepped as one solver (no reference counterpart;
+ * the reference steps one garment per VbdSolver): meshes[k], obstacles[k]
+ * (entries with n_vertices = 0 have none; obstacles may be NULL), x0[k], v0[k]
+ * ([n_k][3]; v0 or v0[k] may be NULL for rest) are concatenated in order.
+ * One colour sweep covers every instance, one detection all of them; the
+ * union's colouring equals each instance's own. The step's query radius and
+ * refresh rule are taken over the whole batch. Instances must be placed so
+ * that none comes within the contact query radius of another. The handle is
+ * a cc_solver: step it, read and write its state (vertices in instance
+ * order) and destroy it with the cc_solver_* calls. */
+int32_t cc_batch_create(const cc_mesh* meshes, const cc_surface* obstacles,
+                        const double* const* x0, const double* const* v0, uint64_t count,
+                        cc_solver** out);
+/* Instance table: first vertex and vertex count of each instance (up to
+ * `capacity` entries written); returns the number of instances (0 for a
+ * solver made by cc_solver_create). */
+uint64_t cc_batch_instances(const cc_solver* solver, uint64_t* first_vertex, uint64_t* vertex_count,
+                            uint64_t capacity);
 /* ------------------------------------------------------ learned guess */
 /* No reference counterpart. A 24-64-64-64-3 GELU MLP predicts, per free
  * vertex, a correction of the adaptive guess from 24 features of the step
