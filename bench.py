@@ -46,6 +46,7 @@ TOLERANCE = 1e-3
 CHECK_EVERY = 2
 ITERATION_CAP = 200
 FIXED_ITERATIONS = 30
+STALL_REFRESH = 2  # refresh the OGC balls after 2 checks without a 5 % residual decrease
 MLP_PATH = os.path.join(ROOT, "clothcraft_b200", "data", "fold_init_mlp.npz")
 UNIT = "steps/s"
 L2_FLUSH_BYTES = 256 << 20
@@ -93,12 +94,14 @@ def config_dict(sc, n_gpus):
         "workload": "sheet256_fold: 256x256 sheet (65,536 v / 130,050 t), 1 m, seeded tilt, dropped onto a "
                     "fixed r=0.3 m icosphere (2,562 v), OGC VF+EE self-contact r=1 mm, k=1e4 N/m, "
                     "dt=1/60 s, StVK-mapped membrane (mu=1e4, lambda=2e4 N/m); iterations until the "
-                    "relative force residual <= 1e-3 (checked every 2, cap 200)",
+                    "relative force residual <= 1e-3 (checked every 2, cap 200, stall refresh after 2 "
+                    "checks without a 5 % decrease)",
         "vertices": int(sc.n),
         "triangles": int(len(sc.mesh.triangles)),
         "residual_tolerance": TOLERANCE,
         "residual_check_every": CHECK_EVERY,
         "iteration_cap": ITERATION_CAP,
+        "stall_refresh": STALL_REFRESH,
         "l2": "flushed between timed steps (256 MiB device write outside the timed events)",
         "phase": "timed steps start at step %d + warm-up (fold phase, contact-rich)" % PHASE_START,
         "parallelism": "replicas x%d (single cloth does not shard)" % n_gpus,
@@ -192,8 +195,10 @@ def step_settings(sc, mode, iterations=None):
     s = sc.settings
     if iterations is None:
         s.iterations, s.residual_tolerance, s.residual_check_every = ITERATION_CAP, TOLERANCE, CHECK_EVERY
+        s.stall_refresh = STALL_REFRESH
     else:
         s.iterations, s.residual_tolerance, s.residual_check_every = iterations, 0.0, 0
+        s.stall_refresh = 0
     s.init_mode = mode
     return s.to_c()
 

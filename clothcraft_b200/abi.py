@@ -82,7 +82,7 @@ class cc_vbd_settings(C.Structure):
         ("contact", cc_ogc_settings),
         ("residual_tolerance", C.c_double),
         ("residual_check_every", C.c_uint32),
-        ("reserved0", C.c_uint32),
+        ("stall_refresh", C.c_uint32),
     ]
 
 

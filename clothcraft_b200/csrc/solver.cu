@@ -81,6 +81,8 @@ struct StepScalars {
     double e_init[2];  // step energy of the adaptive / full-scale learned guess
     int init_used;
     double gx2_iter[256];   // |P grad E(x)|^2 after iteration it (evaluated ones)
+    double stall_best;      // lowest |P grad E|^2 since the last detection (stall refresh)
+    unsigned int stall_count;
     double e_cand, best_e;  // learned-guess scale search
     unsigned int clipped_best;
     int take;
@@ -172,8 +174,11 @@ __global__ void k_refresh_rule(StepScalars* sc, uint32_t it, uint32_t iterations
 // partial sums; with a target, iterations stop at the first evaluation with
 // |grad E(x)| <= tol |grad E(y)|. No reference counterpart (the reference
 // always runs `iterations` sweeps).
+// With `stall` = k > 0, k evaluations in a row without a 5 % decrease of the
+// residual, while vertices are being clipped, request a refresh detection
+// before the next iteration (new OGC balls around the current positions).
 __global__ void __launch_bounds__(256) k_residual_rule(StepScalars* sc, const double* partial, uint32_t it,
-                                                       uint32_t iterations, double tol2, int stop) {
+                                                       uint32_t iterations, double tol2, int stop, uint32_t stall) {
     if (sc->stop_at <= it) return;  // uniform: every thread reads it before thread 0 writes
     double g2 = block_sum_partials(partial);
     if (threadIdx.x == 0) {
@@ -183,6 +188,14 @@ __global__ void __launch_bounds__(256) k_residual_rule(StepScalars* sc, const do
         if (stop && g2 <= tol2 * sc->gy2 && sc->converged_at > it + 1) {
             sc->converged_at = it + 1;
             if (it + 1 < iterations) sc->stop_at = min(sc->stop_at, it + 1);
+        } else if (stop && stall) {
+            if (g2 < 0.9025 * sc->stall_best) {
+                sc->stall_best = g2;
+                sc->stall_count = 0;
+            } else if (++sc->stall_count >= stall && sc->clipped_iter[it] > 0 && it + 1 < iterations) {
+                sc->refresh_at = min(sc->refresh_at, it + 1);
+                sc->stop_at = min(sc->stop_at, it + 1);
+            }
         }
     }
 }
@@ -700,6 +713,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         sv.skip_at = &sc.ptr->stop_at;
         if (lanes == 0) autotune(sv);
         CC_CUDA(cudaMemsetAsync(&sc.ptr->refresh_at, 0xff, 2 * sizeof(unsigned int), stream));  // + converged_at
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->stall_best, 0x7f, sizeof(double), stream));  // ~1.4e306
+        CC_CUDA(cudaMemsetAsync(&sc.ptr->stall_count, 0, sizeof(unsigned int), stream));
         CC_CUDA(cudaMemsetAsync(&sc.ptr->stop_at, 0xff, sizeof(unsigned int), stream));
         CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_iter[it0], 0, (s.iterations - it0) * sizeof(unsigned int), stream));
         const auto& off = coloring.offsets();
@@ -736,7 +751,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                     launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, lanes, true, stream);
                     launch_sum_partial(gsq.ptr, n, partial.ptr, &sc.ptr->stop_at, it, stream);
                     k_residual_rule<<<1, 256, 0, stream>>>(sc.ptr, partial.ptr, it, s.iterations, tol2,
-                                                           target_on ? 1 : 0);
+                                                           target_on ? 1 : 0, s.stall_refresh);
                     own_launches += 3;
                 }
             }

@@ -310,7 +310,7 @@ def capsule(radius: float, height: float, segments: int = 32, rings: int = 8, cy
     c = np.asarray(center, dtype=np.float64)
     rows = []
     half = 0.5 * height
-    for k in range(rings, 0, -1):  # bottom hemisphere, pole excluded
+    for k in range(rings - 1, 0, -1):  # bottom hemisphere, pole excluded
         phi = -0.5 * math.pi * k / rings
         rows.append((radius * math.cos(phi), -half + radius * math.sin(phi)))
     for k in range(cylinder_rings + 1):
@@ -355,6 +355,7 @@ class StepSettings:
     init_mode: int = 0  # 0 adaptive (reference), 1 learned
     residual_tolerance: float = 0.0
     residual_check_every: int = 0
+    stall_refresh: int = 0
 
     def to_c(self) -> abi.cc_vbd_settings:
         s = abi.cc_vbd_settings()
@@ -363,6 +364,7 @@ class StepSettings:
         s.init_mode = self.init_mode
         s.residual_tolerance = self.residual_tolerance
         s.residual_check_every = self.residual_check_every
+        s.stall_refresh = self.stall_refresh
         s.damping = self.damping
         for k in range(3):
             s.gravity[k] = self.gravity[k]

@@ -116,7 +116,12 @@ enum cc_init_mode {
  * residual_check_every = 0: never evaluated (the reference's behaviour).
  * residual_check_every = k > 0: evaluated after every k-th iteration and
  * after the last; with residual_tolerance > 0 the iterations stop at the
- * first evaluation <= residual_tolerance (`iterations` is then the cap). */
+ * first evaluation <= residual_tolerance (`iterations` is then the cap).
+ * stall_refresh = s > 0 (with a tolerance only): after s evaluations in a
+ * row without a 5 % decrease of the residual while vertices are clipped to
+ * their OGC balls, the next iteration starts with a refresh detection, as
+ * the reference's refresh rule does once refresh_fraction * n vertices clip
+ * (src/vbd.rs:326-334); 0 keeps the reference rule alone. */
 typedef struct cc_vbd_settings {
     double dt;
     uint32_t iterations;
@@ -126,7 +131,7 @@ typedef struct cc_vbd_settings {
     cc_ogc_settings contact;
     double residual_tolerance;       /* 0 = run all `iterations`            */
     uint32_t residual_check_every;   /* 0 = no relative residual            */
-    uint32_t reserved0;
+    uint32_t stall_refresh;          /* 0 = off                             */
 } cc_vbd_settings;
 
 /* Grab (src/vbd.rs:54-60): mouse attachment, weights sum to one. */

@@ -56,6 +56,7 @@ VbdSettings to_vbd(const cc_vbd_settings* s) {
     o.contact = to_ogc(&s->contact);
     o.residual_tolerance = s->residual_tolerance;
     o.residual_check_every = s->residual_check_every;
+    o.stall_refresh = s->stall_refresh;
     return o;
 }
 

@@ -282,8 +282,14 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
         metrics.has_relative_residual = true;
     }
     std::vector<Update> updates;
+    double stall_best = HUGE_VAL;
+    size_t stall_count = 0;
+    bool stall_pending = false;
     for (size_t it = 0; it < settings.iterations; ++it) {
-        if (clipped > 0 && (double)clipped >= settings.contact.refresh_fraction * (double)n) {
+        if ((clipped > 0 && (double)clipped >= settings.contact.refresh_fraction * (double)n) || stall_pending) {
+            stall_pending = false;
+            stall_best = HUGE_VAL;
+            stall_count = 0;
             double t = now_ms();
             contacts = world.detect(x, rq, settings.contact);
             colors = this->colors(contacts, grab);
@@ -355,6 +361,14 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
                 gx2 <= settings.residual_tolerance * settings.residual_tolerance * gy2) {
                 metrics.iterations = it + 1;
                 break;
+            }
+            if (settings.residual_tolerance > 0.0 && settings.stall_refresh > 0) {
+                if (gx2 < 0.9025 * stall_best) {
+                    stall_best = gx2;
+                    stall_count = 0;
+                } else if (++stall_count >= settings.stall_refresh && clipped > 0 && it + 1 < settings.iterations) {
+                    stall_pending = true;
+                }
             }
         }
     }

@@ -47,6 +47,7 @@ struct VbdSettings {  // src/vbd.rs:18-52
     // stop at the first evaluation <= tolerance (0 = never stop early).
     double residual_tolerance = 0.0;
     size_t residual_check_every = 0;
+    size_t stall_refresh = 0;  // refresh after this many evaluations without a 5 % decrease
     bool valid() const;
 };
 

@@ -45,11 +45,11 @@ def test_garment_contacts_with_seam_exclusions_match_oracle(garment):
     g = VbdSolver(sc)
     o = oracle.Solver(sc)
     x = sc.x0.copy()
-    # fold each side seam's partners close to each other: stitched pairs are
-    # excluded, every other close pair is a contact
-    n0 = sc.n // 2
+    # bring the back panel to 1.5 mm behind the front one: every stitched
+    # pair sits 1.5 mm apart and is excluded, other close pairs are contacts
     ids = sc.mesh.stitch_vertices.reshape(-1, 2)
-    x[ids[:, 1]] = x[ids[:, 0]] + np.array([0.0, 0.0, -0.0015])
+    n0 = int(ids[0, 1] - ids[0, 0])
+    x[n0:, 2] = x[0, 2] - 0.0015
     xa = g.positions(x)
     cg = g.world.detect(xa, 0.004, sc.settings.ogc_c())
     co = o.world.detect(xa, 0.004, sc.settings.ogc_c())
