@@ -28,13 +28,70 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DATA = os.path.join(HERE, "data")
 
 
-def sample_settings(sc, tolerance: float, cap: int, check: int):
+def sample_settings(sc, tolerance: float, cap: int, check: int, mode: int = 0, stall: int = 2):
     s = sc.settings
     s.iterations = cap
     s.residual_tolerance = tolerance
     s.residual_check_every = check
-    s.init_mode = 0
+    s.stall_refresh = stall
+    s.init_mode = mode
     return s.to_c()
+
+
+def _make_garment(seed):
+    return scenes.config3(seed=seed)
+
+
+def _make_fold(seed):
+    return scenes.config1(seed=seed)
+
+
+def build_scenes(factory, seeds, workers: int = 0):
+    """Scene generation is CPU work (Poisson-disk sampling for garments):
+    spread it over a spawn-started process pool."""
+    if workers <= 1 or len(seeds) <= 1:
+        return [factory(s) for s in seeds]
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(factory, seeds)
+
+
+def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, cap: int = 200, check: int = 2,
+             log=print):
+    """Plain vs learned init at a residual target on each scene: `warm` plain
+    steps, then `steps` steps per init from the same state. Returns a list of
+    per-scene dicts (mean iterations, device ms per step, learned-used fraction)."""
+    out = []
+    for sc in scene_list:
+        g = VbdSolver(sc)
+        g.set_state(sc.x0, sc.v0, 0.0)
+        for _ in range(warm):
+            g.step_resident(sc.settings.to_c())
+        start = g.get_state()
+        row = {"scene": sc.name + ":" + sc.note}
+        for mode, name in ((0, "plain"), (1, "learned")):
+            h = VbdSolver(sc)
+            if mode:
+                h.set_mlp(net, 1)
+            h.set_state(*start)
+            st = sample_settings(sc, tolerance, cap, check, mode)
+            its, ms, used = [], [], []
+            for _ in range(steps):
+                m = h.step_resident(st)
+                its.append(m["iterations"])
+                ms.append(m["gpu_compute_ms"])
+                used.append(m["init_used"])
+            row[name] = {"mean_iterations": float(np.mean(its)), "ms_per_step": float(np.mean(ms)),
+                         "used": float(np.mean(used))}
+        row["time_ratio"] = row["plain"]["ms_per_step"] / row["learned"]["ms_per_step"]
+        row["iteration_ratio"] = row["plain"]["mean_iterations"] / max(row["learned"]["mean_iterations"], 1e-9)
+        log("  %s: plain %.1f it %.2f ms | learned %.1f it %.2f ms (used %.2f) | time x%.2f" % (
+            row["scene"], row["plain"]["mean_iterations"], row["plain"]["ms_per_step"],
+            row["learned"]["mean_iterations"], row["learned"]["ms_per_step"], row["learned"]["used"],
+            row["time_ratio"]), flush=True)
+        out.append(row)
+    return out
 
 
 def collect(scene_list, warm: int, steps: int, tolerance: float = 1e-4, cap: int = 200, check: int = 5,
@@ -75,12 +132,12 @@ def train(features, targets, steps: int = 6000, batch: int = 16384, lr: float = 
     return net, losses
 
 
-def fold_scenes(variants: int, first_seed: int = 2):
-    return [scenes.config1(seed=first_seed + k) for k in range(variants)]
+def fold_scenes(variants: int, first_seed: int = 2, workers: int = 0):
+    return build_scenes(_make_fold, [first_seed + k for k in range(variants)], workers)
 
 
-def garment_scenes(variants: int, first_seed: int = 100):
-    return [scenes.config3(seed=first_seed + k) for k in range(variants)]
+def garment_scenes(variants: int, first_seed: int = 100, workers: int = 0):
+    return build_scenes(_make_garment, [first_seed + k for k in range(variants)], workers)
 
 
 def main(argv=None):
@@ -92,21 +149,41 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--train-steps", type=int, default=6000)
     ap.add_argument("--tolerance", type=float, default=1e-4)
+    ap.add_argument("--workers", type=int, default=min(16, os.cpu_count() or 1))
+    ap.add_argument("--evaluate", type=int, default=0, help="held-out seeds to evaluate on after training")
+    ap.add_argument("--eval-steps", type=int, default=30)
+    ap.add_argument("--weights", default=None, help="skip training: evaluate these weights")
     args = ap.parse_args(argv)
-    if args.kind == "fold":
-        scs = fold_scenes(args.variants or 6)
-        warm, steps = (args.warm if args.warm is not None else 190), (args.steps or 40)
-    else:
-        scs = garment_scenes(args.variants or 50)
-        warm, steps = (args.warm if args.warm is not None else 0), (args.steps or 100)
     out = args.out or os.path.join(DATA, "%s_init_mlp.npz" % args.kind)
-    print("collecting %d variants" % len(scs), flush=True)
-    F, T = collect(scs, warm, steps, tolerance=args.tolerance)
-    net, losses = train(F, T, steps=args.train_steps)
-    os.makedirs(os.path.dirname(out), exist_ok=True)
-    np.savez(out, params=net.parameters(), losses=losses, rows=F.shape[0],
-             scenes=np.array([s.name + ":" + s.note for s in scs]))
-    print("saved", out, flush=True)
+    if args.weights:
+        net = Mlp.load(args.weights)
+    else:
+        if args.kind == "fold":
+            scs = fold_scenes(args.variants or 6, workers=args.workers)
+            warm, steps = (args.warm if args.warm is not None else 190), (args.steps or 40)
+        else:
+            scs = garment_scenes(args.variants or 50, workers=args.workers)
+            warm, steps = (args.warm if args.warm is not None else 0), (args.steps or 100)
+        print("collecting %d variants" % len(scs), flush=True)
+        F, T = collect(scs, warm, steps, tolerance=args.tolerance)
+        net, losses = train(F, T, steps=args.train_steps)
+        del F, T
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        np.savez(out, params=net.parameters(), losses=losses, scenes=np.array([s.name + ":" + s.note for s in scs]))
+        print("saved", out, flush=True)
+    if args.evaluate:
+        if args.kind == "fold":
+            held = fold_scenes(args.evaluate, first_seed=1000, workers=args.workers)
+            warm = 200
+        else:
+            held = garment_scenes(args.evaluate, first_seed=10000, workers=args.workers)
+            warm = 10
+        print("evaluating on %d held-out seeds (tolerance 1e-3)" % len(held), flush=True)
+        rows = evaluate(net, held, warm, args.eval_steps)
+        tr = [r["time_ratio"] for r in rows]
+        ir = [r["iteration_ratio"] for r in rows]
+        print("held-out summary: time ratio plain/learned mean %.3f median %.3f; iteration ratio mean %.3f median %.3f"
+              % (float(np.mean(tr)), float(np.median(tr)), float(np.mean(ir)), float(np.median(ir))), flush=True)
 
 
 if __name__ == "__main__":
