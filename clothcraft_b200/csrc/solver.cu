@@ -346,6 +346,7 @@ struct cc_solver {
     DBuf<uint32_t> st_off, st_v;
     DBuf<double> st_w, st_k;
     DBuf<uint32_t> inc_off, inc, lo_off, lo;
+    DBuf<uint2> inc_mid;  // per vertex: first hinge entry, first stitch entry
     DBuf<uint8_t> pinned;
     DBuf<double> masses;
     // state and per-step buffers
@@ -420,6 +421,7 @@ struct cc_solver {
         v.inertia = inertia.ptr;
         v.pinned = pinned.ptr;
         v.inc_off = inc_off.ptr;
+        v.inc_mid = inc_mid.ptr;
         v.inc = inc.ptr;
         v.tri_v = tri_v.ptr;
         v.tri_coef = tri_coef.ptr;
@@ -1074,8 +1076,17 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
             connect(ids.data(), ids.size());
         }
         std::vector<uint32_t> io(n + 1, 0), iv, lo_o(n + 1, 0), lo_v;
+        std::vector<uint2> mid(n);
         for (uint64_t v = 0; v < n; ++v) {
             io[v + 1] = io[v] + (uint32_t)inc[v].size();
+            // entries are grouped by type (triangles, hinges, stitches): record the boundaries
+            uint32_t hb = io[v], sb = io[v];
+            for (uint32_t e : inc[v]) {
+                uint32_t type = e >> 30;
+                if (type == TERM_TRI) ++hb, ++sb;
+                else if (type == TERM_HINGE) ++sb;
+            }
+            mid[v] = make_uint2(hb, sb);
             iv.insert(iv.end(), inc[v].begin(), inc[v].end());
             for (uint32_t u : graph[v])
                 if (u < v) lo_v.push_back(u);
@@ -1110,6 +1121,7 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         h->st_w.upload(sw, st);
         h->st_k.upload(sk, st);
         h->inc_off.upload(io, st);
+        h->inc_mid.upload(mid, st);
         h->inc.upload(iv, st);
         h->lo_off.upload(lo_o, st);
         h->lo.upload(lo_v, st);

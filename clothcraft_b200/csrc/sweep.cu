@@ -478,14 +478,18 @@ __device__ __forceinline__ double grab_term(const SweepView& s, uint32_t v, d3 p
 template <bool D, int G>
 __device__ __forceinline__ double local_part(const SweepView& s, uint32_t v, d3 p, uint32_t lane, d3& g, Sym& H) {
     double e = 0.0;
-    uint32_t b1 = s.inc_off[v + 1];
-    for (uint32_t k = s.inc_off[v] + lane; k < b1; k += G) {
+    // entries are grouped by type: one lane-strided loop per type, no per-entry dispatch
+    uint32_t b0 = s.inc_off[v], b1 = s.inc_off[v + 1];
+    uint2 mid = s.inc_mid[v];
+    for (uint32_t k = b0 + lane; k < mid.x; k += G) {
         uint32_t ent = s.inc[k];
-        uint32_t type = ent >> 30, slot = (ent >> 28) & 3u, idx = ent & 0x0fffffffu;
-        if (type == TERM_TRI) e += membrane_term<D>(s, idx, slot, p, g, H);
-        else if (type == TERM_HINGE) e += bending_term<D>(s, idx, slot, p, g, H);
-        else e += stitch_term<D>(s, idx, v, p, g, H);
+        e += membrane_term<D>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
     }
+    for (uint32_t k = mid.x + lane; k < mid.y; k += G) {
+        uint32_t ent = s.inc[k];
+        e += bending_term<D>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
+    }
+    for (uint32_t k = mid.y + lane; k < b1; k += G) e += stitch_term<D>(s, s.inc[k] & 0x0fffffffu, v, p, g, H);
     uint32_t c1 = s.contacts.inc_off[v + 1];
     for (uint32_t k = s.contacts.inc_off[v] + lane; k < c1; k += G) e += contact_term<D>(s, s.contacts.inc[k], v, p, g, H);
     if (lane == 0 && s.grab.active && (s.grab.v[0] == v || s.grab.v[1] == v || s.grab.v[2] == v))

@@ -29,6 +29,7 @@ struct SweepView {
     const double* inertia;      // [n]
     const uint8_t* pinned;      // [n]
     const uint32_t* inc_off;    // [n+1] static incidence
+    const uint2* inc_mid;       // [n] first hinge entry, first stitch entry (entries grouped by type)
     const uint32_t* inc;
     const int4* tri_v;          // v0, v1, v2, material
     const double4* tri_coef;    // w = ds0*c.x + ds1*c.y ; v = ds0*c.z + ds1*c.w (grain-rotated inv_dm)

@@ -223,15 +223,45 @@ static std::vector<double> sys_diagonal(const NSystem& s, double shift, size_t n
     return d;
 }
 
-static std::vector<double> sys_apply(const NSystem& s, const std::vector<double>& x, double shift, size_t n) {
-    std::vector<double> out(3 * n);
-    for (size_t i = 0; i < 3 * n; ++i) out[i] = x[i] * (s.mass_diag[i] + shift);
+// Elements incident to each vertex, in element order (item = element << 2 | slot),
+// so that the product can be gathered per row in parallel with the same
+// summation order as the element-by-element scatter.
+struct VertexElements {
+    std::vector<size_t> off;
+    std::vector<uint64_t> item;
+};
+static VertexElements vertex_elements(const NSystem& s, size_t n) {
+    VertexElements g;
+    g.off.assign(n + 1, 0);
     for (const NElement& e : s.elements)
-        for (int a = 0; a < e.nv; ++a) {
-            if (e.verts[a] >= n) continue;
-            for (int ka = 0; ka < 3; ++ka) {
-                size_t gi = 3 * e.verts[a] + ka;
-                if (s.fixed[gi]) continue;
+        for (int a = 0; a < e.nv; ++a)
+            if (e.verts[a] < n) ++g.off[e.verts[a] + 1];
+    for (size_t i = 0; i < n; ++i) g.off[i + 1] += g.off[i];
+    g.item.resize(g.off[n]);
+    std::vector<size_t> fill(g.off.begin(), g.off.end() - 1);
+    for (size_t k = 0; k < s.elements.size(); ++k) {
+        const NElement& e = s.elements[k];
+        for (int a = 0; a < e.nv; ++a)
+            if (e.verts[a] < n) g.item[fill[e.verts[a]]++] = ((uint64_t)k << 2) | (uint64_t)a;
+    }
+    return g;
+}
+
+static std::vector<double> sys_apply(const NSystem& s, const VertexElements& g, const std::vector<double>& x,
+                                     double shift, size_t n, int threads) {
+    std::vector<double> out(3 * n);
+#pragma omp parallel for num_threads(threads) schedule(static, 256)
+    for (size_t v = 0; v < n; ++v) {
+        for (int ka = 0; ka < 3; ++ka) {
+            size_t gi = 3 * v + ka;
+            if (s.fixed[gi]) {
+                out[gi] = x[gi];
+                continue;
+            }
+            double o = x[gi] * (s.mass_diag[gi] + shift);
+            for (size_t q = g.off[v]; q < g.off[v + 1]; ++q) {
+                const NElement& e = s.elements[g.item[q] >> 2];
+                int a = (int)(g.item[q] & 3u);
                 double acc = 0.0;
                 for (int b = 0; b < e.nv; ++b) {
                     if (e.verts[b] >= n) continue;
@@ -240,15 +270,16 @@ static std::vector<double> sys_apply(const NSystem& s, const std::vector<double>
                         if (!s.fixed[gj]) acc += e.h[(3 * a + ka) * 12 + 3 * b + kb] * x[gj];
                     }
                 }
-                out[gi] += acc;
+                o += acc;
             }
+            out[gi] = o;
         }
-    for (size_t i = 0; i < 3 * n; ++i)
-        if (s.fixed[i]) out[i] = x[i];
+    }
     return out;
 }
 
-static bool sys_pcg(const NSystem& s, double shift, size_t limit, size_t n, std::vector<double>& x, size_t& its) {
+static bool sys_pcg(const NSystem& s, const VertexElements& g, double shift, size_t limit, size_t n,
+                    std::vector<double>& x, size_t& its, int threads) {
     std::vector<double> diag = sys_diagonal(s, shift, n);
     x.assign(3 * n, 0.0);
     std::vector<double> r(3 * n), z(3 * n), p(3 * n);
@@ -258,7 +289,7 @@ static bool sys_pcg(const NSystem& s, double shift, size_t limit, size_t n, std:
     double rz = vdot_(r, z);
     double tol = 1e-5 * std::sqrt(vdot_(r, r));
     for (size_t it = 0; it < limit; ++it) {
-        std::vector<double> ap = sys_apply(s, p, shift, n);
+        std::vector<double> ap = sys_apply(s, g, p, shift, n, threads);
         double curv = vdot_(p, ap);
         if (!std::isfinite(curv) || curv <= 0.0) {
             its = it + 1;
@@ -321,13 +352,14 @@ NewtonResult newton_step(const NewtonInput& in, int newton_iterations, size_t pc
         if (iteration == newton_iterations) break;
         double scale = 1.0;
         for (double d : sys_diagonal(sys, 0.0, n)) scale = std::fmax(scale, d);
+        VertexElements elems = vertex_elements(sys, n);
         bool accepted = false;
         std::vector<D3> trial;
         double shift = 0.0;
         for (int attempt = 0; attempt < 12 && !accepted; ++attempt) {
             std::vector<double> dir;
             size_t its = 0;
-            bool ok = sys_pcg(sys, shift, pcg_iterations, n, dir, its);
+            bool ok = sys_pcg(sys, elems, shift, pcg_iterations, n, dir, its, threads);
             out.pcg_iterations += its;
             if (ok) {
                 double slope = vdot_(sys.gradient, dir);
