@@ -291,30 +291,44 @@ __device__ __forceinline__ S activation(const S& d, double r, double k) {
     return scst<S>(0.5 * k * tau * tau) - scst<S>(k * tau * tau) * sln(d / scst<S>(tau));
 }
 
-// Contact::energy (src/ogc/potential.rs:39-65) on four named points.
+// Contact distance of Contact::energy (src/ogc/potential.rs:39-65) on four
+// named points; `degenerate` is set for an EE pair with |n|^2 < 1e-30 (energy 0).
 template <class S>
-__device__ __forceinline__ S contact_energy_t(uint32_t kind, double eps, const V<S>& p0, const V<S>& p1,
-                                              const V<S>& p2, const V<S>& p3, double r, double k) {
-    S d;
+__device__ __forceinline__ S contact_distance(uint32_t kind, const V<S>& p0, const V<S>& p1, const V<S>& p2,
+                                              const V<S>& p3, bool& degenerate) {
+    degenerate = false;
     if (kind == 0) {
         V<S> v = vsub(p0, p1);
-        d = ssqrt(vdot(v, v));
-    } else if (kind == 1) {
+        return ssqrt(vdot(v, v));
+    }
+    if (kind == 1) {
         V<S> u = vsub(p2, p1);
         V<S> w = vsub(p0, p1);
         S q = vdot(w, u) / vdot(u, u);
         V<S> dd = {w.x - q * u.x, w.y - q * u.y, w.z - q * u.z};
-        d = ssqrt(vdot(dd, dd));
-    } else if (kind == 2) {
+        return ssqrt(vdot(dd, dd));
+    }
+    if (kind == 2) {
         V<S> n = vcross(vsub(p2, p1), vsub(p3, p1));
         S h = vdot(vsub(p0, p1), n) / ssqrt(vdot(n, n));
-        d = sval(h) < 0.0 ? -h : h;
-    } else {
-        V<S> n = vcross(vsub(p1, p0), vsub(p3, p2));
-        if (sval(vdot(n, n)) < 1e-30) return scst<S>(0.0);
-        S h = vdot(vsub(p0, p2), n) / ssqrt(vdot(n, n));
-        d = sval(h) < 0.0 ? -h : h;
+        return sval(h) < 0.0 ? -h : h;
     }
+    V<S> n = vcross(vsub(p1, p0), vsub(p3, p2));
+    if (sval(vdot(n, n)) < 1e-30) {
+        degenerate = true;
+        return scst<S>(0.0);
+    }
+    S h = vdot(vsub(p0, p2), n) / ssqrt(vdot(n, n));
+    return sval(h) < 0.0 ? -h : h;
+}
+
+// Contact::energy (src/ogc/potential.rs:39-65) on four named points.
+template <class S>
+__device__ __forceinline__ S contact_energy_t(uint32_t kind, double eps, const V<S>& p0, const V<S>& p1,
+                                              const V<S>& p2, const V<S>& p3, double r, double k) {
+    bool degenerate;
+    S d = contact_distance<S>(kind, p0, p1, p2, p3, degenerate);
+    if (degenerate) return scst<S>(0.0);
     S e = activation(d, r, k);
     if (kind == 3) {
         V<S> n = vcross(vsub(p1, p0), vsub(p3, p2));
@@ -429,6 +443,12 @@ __device__ __forceinline__ double contact_term(const SweepView& s, uint32_t c, u
     uint4 cv = s.contacts.verts[c];
     double eps = s.contacts.eps[c];
     if (D) {
+        // Inactive term (d >= r): the activation is the constant 0, so the term
+        // adds nothing to e, g or H; skip its derivative evaluation.
+        bool degenerate;
+        double d0 = contact_distance<double>(kind, dpoint(s, cv.x, v, p), dpoint(s, cv.y, v, p),
+                                             dpoint(s, cv.z, v, p), dpoint(s, cv.w, v, p), degenerate);
+        if (degenerate || d0 >= s.contact_r) return 0.0;
         // the moving vertex's slot among the used ones (unused slots hold 0)
         uint32_t cnt = kind == 0 ? 2u : (kind == 1 ? 3u : 4u);
         int slot = cv.x == v ? 0 : (cv.y == v ? 1 : ((cnt > 2 && cv.z == v) ? 2 : 3));

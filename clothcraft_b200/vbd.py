@@ -259,6 +259,14 @@ class VbdSolver:
         if rc != 0:
             raise self._err(rc)
 
+    def set_lanes(self, lanes: int):
+        """Threads per vertex solve (1..32), or 0 to autotune on the next step.
+        Two solvers give bitwise-identical steps only with the same lanes."""
+        rc = native.load().cc_solver_set_lanes(self.h, int(lanes))
+        if rc != 0:
+            raise self._err(rc)
+        return self
+
     def last_step_trace(self):
         """(relative residual after each iteration, NaN where not evaluated;
         vertices clipped in each iteration) of the last step."""

@@ -136,7 +136,7 @@ def _plain_and_learned(net, precision, steps=3):
     s = sc.settings
     s.init_mode = 1
     st_l = s.to_c()
-    a, b = VbdSolver(sc), VbdSolver(sc)
+    a, b = VbdSolver(sc).set_lanes(4), VbdSolver(sc).set_lanes(4)  # bitwise comparison: same lanes
     b.set_mlp(net, precision)
     x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
     xb, vb, tb = x.copy(), v.copy(), t

@@ -84,11 +84,11 @@ def test_residual_target_stops_at_first_evaluation_below_it():
         res[k] = m["relative_residual"]
     tol = 0.5 * (res[6] + res[8])  # met first at k = 8
     assert res[6] > tol >= res[8]
-    g = VbdSolver(sc)
+    g = VbdSolver(sc).set_lanes(4)  # bitwise comparison: same lanes in both solvers
     xa, va, _, ma = g.step(x0, v0, t0, settings(sc, 60, check=2, tol=tol).to_c())
     assert ma["iterations"] == 8
     assert ma["relative_residual"] <= tol
-    g2 = VbdSolver(sc)
+    g2 = VbdSolver(sc).set_lanes(4)
     xb, vb, _, mb = g2.step(x0, v0, t0, settings(sc, 8, check=2).to_c())
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
     assert ma["relative_residual"] == mb["relative_residual"]
@@ -102,13 +102,13 @@ def test_residual_target_on_the_fold_state_with_refreshes():
     z = np.load(scenes_fold_state())
     x0, v0 = z["x"].astype(np.float64), z["v"].astype(np.float64)
     t0 = 200 / 60
-    g = VbdSolver(sc)
+    g = VbdSolver(sc).set_lanes(4)  # bitwise comparison: same lanes in both solvers
     g.set_state(x0, v0, t0)
     ma = g.step_resident(settings(sc, 120, check=5, tol=2e-3).to_c())
     xa, va, _ = g.get_state()
     k = ma["iterations"]
     assert k % 5 == 0 and ma["relative_residual"] <= 2e-3 or k == 120
-    g2 = VbdSolver(sc)
+    g2 = VbdSolver(sc).set_lanes(4)
     g2.set_state(x0, v0, t0)
     mb = g2.step_resident(settings(sc, k, check=5).to_c())
     xb, vb, _ = g2.get_state()

@@ -204,8 +204,8 @@ def test_invalid_settings_and_state_are_rejected_on_gpu():
 def test_resident_stepping_equals_host_stepping():
     sc = contact_scene(12, seed=8)
     st = sc.settings.to_c()
-    a = VbdSolver(sc)
-    b = VbdSolver(sc)
+    a = VbdSolver(sc).set_lanes(4)  # bitwise comparison: same lanes in both solvers
+    b = VbdSolver(sc).set_lanes(4)
     x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
     b.set_state(x, v, t)
     for _ in range(5):
