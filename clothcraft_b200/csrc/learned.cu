@@ -13,9 +13,7 @@
 //   17    100 * max principal fibre strain max(E_ww, E_ff)
 //   18    OGC nearest distance / query radius (radius / relaxation / rq)
 //   19    contact terms incident to the vertex / 4 (capped at 16)
-//   20    (v0 dt . normal) / u
-//   21    |y - guess| / u
-//   22    mass / mean mass - 1
+//   20-22 last step's correction (x_end - adaptive guess) / u, 0 without history
 //   23    1 - ring size / 6
 // The network maps them to a correction c; the learned guess is
 // guess + u * c, clipped to the vertex's OGC ball.
@@ -47,7 +45,7 @@ __global__ void k_features(FeatureView f, float* out) {
         if (f.pinned[v]) continue;
         float* o = out + (size_t)f.row[v] * kMlpIn;
         const double iu = 1.0 / f.unit;
-        d3 x = ld3(f.x0, v), y = ld3(f.target, v), g = ld3(f.guess, v), vel = ld3(f.v0, v);
+        d3 x = ld3(f.x0, v), y = ld3(f.target, v), g = ld3(f.guess, v);
         d3 dy = (y - x) * iu, dg = (g - x) * iu;
         d3 nb_dg = mk(0, 0, 0), nb_x = mk(0, 0, 0);
         double elen = 0.0;
@@ -97,8 +95,8 @@ __global__ void k_features(FeatureView f, float* out) {
         }
         double dmin = f.contacts.radii[v] / f.relaxation / f.query_radius;
         uint32_t nc = f.contacts.inc_off[v + 1] - f.contacts.inc_off[v];
-        double vn = dot(vel * f.dt, nrm) * iu;
-        double yg = len(y - g) * iu;
+        d3 pc = mk(0, 0, 0);
+        if (f.history && *f.mismatch == 0) pc = ld3(f.prev_corr, v) * iu;
         double feat[kMlpIn] = {dy.x,
                                dy.y,
                                dy.z,
@@ -119,9 +117,9 @@ __global__ void k_features(FeatureView f, float* out) {
                                100.0 * mx,
                                fmin(dmin, 1.0),
                                (double)min(nc, 16u) * 0.25,
-                               vn,
-                               yg,
-                               f.masses[v] / f.mean_mass - 1.0,
+                               pc.x,
+                               pc.y,
+                               pc.z,
                                1.0 - (double)cnt / 6.0};
 #pragma unroll
         for (int k = 0; k < kMlpIn; ++k) o[k] = (float)feat[k];

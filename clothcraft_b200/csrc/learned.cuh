@@ -47,6 +47,9 @@ struct FeatureView {
     double dt;
     double unit;  // displacement unit |g| dt^2
     const uint32_t* row;  // [n] output row of each free vertex
+    const double4* prev_corr;      // [n] last step's x_end - adaptive guess
+    int history;                   // host side of the adaptive-guess history test
+    const unsigned int* mismatch;  // device side (state edited since the last step)
 };
 
 // out[row[v]][24] for every free vertex v.

@@ -243,9 +243,10 @@ __global__ void k_step_finish(uint32_t n, const double4* x, ContactsView c, cons
 
 // commit + Prediction::record (src/vbd.rs:406-411, prediction.rs:43-54)
 __global__ void k_commit(uint32_t n, const double4* x, double4* x0, double4* v0, double4* px, double4* pv,
-                         double4* accel, double dt, double damping) {
+                         double4* accel, double dt, double damping, const double4* guess, double4* prev_corr) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         d3 p = ld3(x, i), xo = ld3(x0, i), vo = ld3(v0, i);
+        st3(prev_corr, i, p - ld3(guess, i));  // learned-guess feature of the next step
         d3 v = (p - xo) / dt;
         st3(x0, i, p);
         st3(v0, i, v);
@@ -385,7 +386,8 @@ struct cc_solver {
     DBuf<uint32_t> ring_off, ring, row;
     double mean_mass = 1.0;
     DBuf<float> feat, corr;
-    DBuf<double4> best;
+    DBuf<double4> best, prev_corr;
+    bool step_history = false;  // the adaptive-guess history test of the current step (host part)
     float* sample_features = nullptr;  // caller device buffers of cc_solver_step_sample
     float* sample_targets = nullptr;
     cudaEvent_t learn0 = nullptr, learn1 = nullptr;
@@ -507,6 +509,9 @@ struct cc_solver {
         double g = std::sqrt(s.gravity[0] * s.gravity[0] + s.gravity[1] * s.gravity[1] + s.gravity[2] * s.gravity[2]);
         f.unit = g * s.dt * s.dt > 1e-9 ? g * s.dt * s.dt : 1e-3;
         f.row = row.ptr;
+        f.prev_corr = prev_corr.ptr;
+        f.history = step_history ? 1 : 0;
+        f.mismatch = &sc.ptr->mismatch;
         return f;
     }
     void learned_guess(const cc_vbd_settings& s, const cc_grab* grab, const ContactsView& cv, double rq,
@@ -634,6 +639,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     k_step_begin<<<gb, 256, 0, stream>>>(n, x0.ptr, v0.ptr, pred_x.ptr, pred_v.ptr, has_pred ? 1 : 0, sc.ptr);
     bool history = has_pred && pred_time == time && pred_g[0] == s.gravity[0] && pred_g[1] == s.gravity[1] &&
                    pred_g[2] == s.gravity[2] && pred_damping == s.damping;
+    step_history = history;
     double3 g3 = make_double3(s.gravity[0], s.gravity[1], s.gravity[2]);
     k_predict<<<gb, 256, 0, stream>>>(n, x0.ptr, v0.ptr, accel.ptr, history ? 1 : 0, sc.ptr, s.dt, g3, s.damping,
                                       masses.ptr, guess.ptr, target.ptr, inertia.ptr, sc.ptr);
@@ -816,7 +822,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     m.residual_rms_n = std::sqrt(sc_h.ptr->residual / (double)(3 * (size_t)n));
     m.has_residual = 1;
     k_commit<<<gb, 256, 0, stream>>>(n, world->x(), x0.ptr, v0.ptr, pred_x.ptr, pred_v.ptr, accel.ptr, s.dt,
-                                     s.damping);
+                                     s.damping, guess.ptr, prev_corr.ptr);
     ++own_launches;
     time += s.dt;
     has_pred = true;
@@ -1139,7 +1145,8 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         CC_CUDA(cudaEventCreate(&h->learn0));
         CC_CUDA(cudaEventCreate(&h->learn1));
         h->masses.upload(mesh->masses, n, st);
-        for (auto* b : {&h->x0, &h->v0, &h->guess, &h->target, &h->pred_x, &h->pred_v, &h->accel}) b->reserve(n);
+        for (auto* b : {&h->x0, &h->v0, &h->guess, &h->target, &h->pred_x, &h->pred_v, &h->accel, &h->prev_corr})
+            b->reserve(n);
         h->inertia.reserve(n);
         h->residual.reserve(n);
         h->clipped_flag.reserve(n);

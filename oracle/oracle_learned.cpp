@@ -153,6 +153,7 @@ int32_t or_learned_features(or_solver* h, const double* x, const double* v, doub
         vs.contact.relaxation = st->contact.relaxation;
         vs.contact.refresh_fraction = st->contact.refresh_fraction;
         std::vector<D3> guess = s.prediction.guess(state, vs);
+        const bool history = s.prediction.valid(state, vs) && s.last_guess.size() == n;
         double damp = 1.0 + vs.damping * vs.dt;
         std::vector<D3> y(n);
         double motion = 0.0;
@@ -173,9 +174,6 @@ int32_t or_learned_features(or_solver* h, const double* x, const double* v, doub
                     if (a != b) ring[tv[a]].insert(tv[b]);
             }
         }
-        double msum = 0.0;
-        for (double m : mesh.masses) msum += m;
-        double mean_mass = n ? msum / (double)n : 1.0;
         double g = length(vs.gravity);
         double unit = g * vs.dt * vs.dt > 1e-9 ? g * vs.dt * vs.dt : 1e-3;
         size_t row = 0;
@@ -223,6 +221,8 @@ int32_t or_learned_features(or_solver* h, const double* x, const double* v, doub
             }
             double dmin = cs.radii[vtx] / vs.contact.relaxation / rq;
             size_t nc = cs.incident[vtx].size();
+            D3 pc{0, 0, 0};
+            if (history) pc = (xv - s.last_guess[vtx]) / unit;
             double feat[kIn] = {dy.x,
                                 dy.y,
                                 dy.z,
@@ -243,9 +243,9 @@ int32_t or_learned_features(or_solver* h, const double* x, const double* v, doub
                                 100.0 * mx,
                                 std::fmin(dmin, 1.0),
                                 (double)std::min<size_t>(nc, 16) * 0.25,
-                                dot(state.v[vtx] * vs.dt, nrm) / unit,
-                                length(y[vtx] - guess[vtx]) / unit,
-                                mesh.masses[vtx] / mean_mass - 1.0,
+                                pc.x,
+                                pc.y,
+                                pc.z,
                                 1.0 - (double)cnt / 6.0};
             for (int k = 0; k < kIn; ++k) out[row * kIn + k] = (float)feat[k];
             ++row;

@@ -19,14 +19,19 @@ bool VbdSettings::valid() const {  // src/vbd.rs:38-51
 }
 
 // src/vbd/prediction.rs:15-41
-std::vector<D3> Prediction::guess(const State& state, const VbdSettings& s) const {
-    bool valid = false;
+bool Prediction::valid(const State& state, const VbdSettings& s) const {
+    bool ok = false;
     if (has_last) {
-        valid = last.time == state.time && last.x.size() == state.x.size() && last.v.size() == state.v.size() &&
-                gravity == s.gravity && damping == s.damping;
-        for (size_t i = 0; valid && i < state.x.size(); ++i) valid = last.x[i] == state.x[i];
-        for (size_t i = 0; valid && i < state.v.size(); ++i) valid = last.v[i] == state.v[i];
+        ok = last.time == state.time && last.x.size() == state.x.size() && last.v.size() == state.v.size() &&
+             gravity == s.gravity && damping == s.damping;
+        for (size_t i = 0; ok && i < state.x.size(); ++i) ok = last.x[i] == state.x[i];
+        for (size_t i = 0; ok && i < state.v.size(); ++i) ok = last.v[i] == state.v[i];
     }
+    return ok;
+}
+
+std::vector<D3> Prediction::guess(const State& state, const VbdSettings& s) const {
+    bool valid = this->valid(state, s);
     double g2 = length_squared(s.gravity);
     std::vector<D3> out(state.x.size());
     for (size_t i = 0; i < state.x.size(); ++i) {
@@ -383,6 +388,7 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
     }
     state.time += dt;
     prediction.record(old_velocity, state, settings);
+    last_guess = guess;
     metrics.time_s = state.time;
     metrics.contacts = contacts.active_contacts;
     metrics.contact_terms = contacts.contacts.size();

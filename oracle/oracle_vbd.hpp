@@ -83,11 +83,14 @@ struct Prediction {  // src/vbd/prediction.rs:6-54
     D3 gravity{0, 0, 0};
     double damping = 0;
     std::vector<D3> guess(const State& state, const VbdSettings& s) const;
+    // the history test of guess(): the state is the one last recorded
+    bool valid(const State& state, const VbdSettings& s) const;
     void record(const std::vector<D3>& old_velocity, const State& state, const VbdSettings& s);
 };
 
 struct VbdSolver {  // src/vbd.rs:89-99
     Prediction prediction;
+    std::vector<D3> last_guess;  // adaptive guess of the last step (learned-guess feature)
     Mesh mesh;
     OgcWorld world;
     std::vector<std::vector<uint32_t>> triangles, hinges, vertex_stitches, graph;

@@ -39,6 +39,6 @@ def test_features_layout_on_a_resting_sheet():
     # at rest with a fresh history: inertial displacement = guess = g dt^2 / (1 + c dt) / u
     expect = -1.0 / (1.0 + st.damping * st.dt)
     assert np.allclose(F[:, 1], expect, rtol=1e-6) and np.allclose(F[:, 4], expect, rtol=1e-6)
-    assert np.allclose(F[:, 21], 0.0)  # |y - guess| = 0 without history
+    assert np.allclose(F[:, 20:23], 0.0)  # no last-step correction without history
     assert np.allclose(np.abs(F[:, 13]), 1.0, atol=1e-6)  # flat sheet: normal along y
     assert np.all(F[:, 18] <= 1.0) and np.all(F[:, 18] > 0.0)
