@@ -76,7 +76,8 @@ __device__ __forceinline__ d3 pos(const SweepView& s, uint32_t i, uint32_t v, d3
 }
 
 // membrane (src/energy.rs:17-29) of triangle t with vertex slot `slot` at p.
-template <bool D>
+// D: derivatives; HS: also the Hessian (a gradient-only evaluation skips it)
+template <bool D, bool HS = D>
 __device__ __forceinline__ double membrane_term(const SweepView& s, uint32_t t, uint32_t slot, d3 p, d3& g, Sym& H) {
     int4 tv = s.tri_v[t];
     double4 cf = s.tri_coef[t];
@@ -99,6 +100,7 @@ __device__ __forceinline__ double membrane_term(const SweepView& s, uint32_t t, 
     double av = slot == 0 ? -(cf.z + cf.w) : (slot == 1 ? cf.z : cf.w);
     d3 q = v * aw + w * av;
     g = g + (w * (fw1 * aw) + v * (fv1 * av) + q * (M.shear * sh)) * A;
+    if (!HS) return A * (fw + fv + 0.5 * M.shear * sh * sh);
     sym_add_outer(H, w, A * fw2 * aw * aw);
     sym_add_outer(H, v, A * fv2 * av * av);
     sym_add_outer(H, q, A * M.shear);
@@ -129,7 +131,7 @@ __device__ __forceinline__ void add_curvature(Sym& Hm, d3 a, d3 h, d3 d, double 
 
 // bending (src/energy.rs:31-46) of hinge h with vertex slot `slot` at p.
 // n1 = e x u, n2 = w x e are affine in one vertex: dn_k/dp = [a_k]x.
-template <bool D>
+template <bool D, bool HS = D>
 __device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, uint32_t slot, d3 p, d3& g, Sym& H) {
     uint4 hv = s.hinge_v[hi];
     double K = s.hinge_k[hi];
@@ -152,6 +154,7 @@ __device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, 
     d3 pd1 = d - h1 * dot(h1, d), pd2 = d - h2 * dot(h2, d);
     d3 jtd = cross(pd1, a1) * il1 - cross(pd2, a2) * il2;
     g = g + jtd * (2.0 * K);
+    if (!HS) return energy;
     // Hessian 2K [J^T J + A1^T M1 A1 - A2^T M2 A2]
     d3 c0 = mk(0, 0, 0), c1 = mk(0, 0, 0), c2 = mk(0, 0, 0);
     proj_skew_cols(a1, h1, il1, 1.0, c0, c1, c2);
@@ -495,7 +498,7 @@ __device__ __forceinline__ double grab_term(const SweepView& s, uint32_t v, d3 p
 
 // Partial sum of the incident terms dealt to `lane` of a group of G
 // (VbdSolver::local, src/vbd.rs:196-248).
-template <bool D, int G>
+template <bool D, int G, bool HS = D>
 __device__ __forceinline__ double local_part(const SweepView& s, uint32_t v, d3 p, uint32_t lane, d3& g, Sym& H) {
     double e = 0.0;
     // entries are grouped by type: one lane-strided loop per type, no per-entry dispatch
@@ -503,11 +506,11 @@ __device__ __forceinline__ double local_part(const SweepView& s, uint32_t v, d3 
     uint2 mid = s.inc_mid[v];
     for (uint32_t k = b0 + lane; k < mid.x; k += G) {
         uint32_t ent = s.inc[k];
-        e += membrane_term<D>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
+        e += membrane_term<D, HS>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
     }
     for (uint32_t k = mid.x + lane; k < mid.y; k += G) {
         uint32_t ent = s.inc[k];
-        e += bending_term<D>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
+        e += bending_term<D, HS>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
     }
     for (uint32_t k = mid.y + lane; k < b1; k += G) e += stitch_term<D>(s, s.inc[k] & 0x0fffffffu, v, p, g, H);
     uint32_t c1 = s.contacts.inc_off[v + 1];
@@ -697,7 +700,7 @@ __global__ void __launch_bounds__(128) k_grad_sq(SweepView s, double* out, const
     d3 g = mk(0, 0, 0);
     Sym H;
     sym_zero(H);
-    local_part<true, G>(s, v, x, lane, g, H);
+    local_part<true, G, false>(s, v, x, lane, g, H);  // gradient only
     if (G > 1) {
         g.x = group_sum<G>(g.x, mask);
         g.y = group_sum<G>(g.y, mask);
