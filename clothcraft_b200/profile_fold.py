@@ -1,0 +1,53 @@
+"""Run a few steps of the benchmark workload for a profiler.
+
+  python -m clothcraft_b200.profile_fold [--steps 2] [--lanes 4] [--learned] [--fixed N]
+
+The 256x256 self-contact fold from its committed fold-phase state
+(tests/golden/sheet256_fold_state.npz), stepped to the benchmark's residual
+target (1e-3, checked every 2 iterations, stall refresh 2, cap 200), or a
+fixed iteration count with --fixed. Nothing is timed here: wrap it in
+`ncu` to see the launches of exactly this workload.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+
+import numpy as np
+
+from . import scenes
+from .vbd import VbdSolver
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FOLD_STATE = os.path.join(os.path.dirname(HERE), "tests", "golden", "sheet256_fold_state.npz")
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--lanes", type=int, default=4)
+    ap.add_argument("--learned", action="store_true")
+    ap.add_argument("--fixed", type=int, default=0)
+    args = ap.parse_args(argv)
+    sc = scenes.config1()
+    z = np.load(FOLD_STATE)
+    g = VbdSolver(sc).set_lanes(args.lanes)
+    s = sc.settings
+    if args.fixed:
+        s.iterations = args.fixed
+    else:
+        s.iterations, s.residual_tolerance, s.residual_check_every, s.stall_refresh = 200, 1e-3, 2, 2
+    if args.learned:
+        from .learned import Mlp
+
+        g.set_mlp(Mlp.load(os.path.join(HERE, "data", "fold_init_mlp.npz")), 1)
+        s.init_mode = 1
+    g.set_state(z["x"].astype(np.float64), z["v"].astype(np.float64), float(z["time"]))
+    for k in range(args.steps):
+        m = g.step_resident(s.to_c())
+        print("step %d: %d iterations, %.2f ms, residual %s" % (k, m["iterations"], m["gpu_compute_ms"],
+                                                              m["relative_residual"]), flush=True)
+
+
+if __name__ == "__main__":
+    main()
