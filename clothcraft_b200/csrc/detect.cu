@@ -186,7 +186,7 @@ __global__ void k_karras(const unsigned long long* code, int m, int2* child, int
 }
 
 __global__ void k_lbvh_boxes(const Box* prim_box, const uint32_t* leaf_prim, int m, const int2* child,
-                             const int* parent, unsigned* visits, Box* node_box) {
+                             const int* parent, unsigned* visits, Box* node_box, uint32_t* node_max) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         int node = parent[m - 1 + i];
         while (node >= 0) {
@@ -195,7 +195,10 @@ __global__ void k_lbvh_boxes(const Box* prim_box, const uint32_t* leaf_prim, int
             int2 c = child[node];
             Box a = (c.x & 0x80000000) ? prim_box[leaf_prim[c.x & 0x7fffffff]] : ldcg_box(&node_box[c.x]);
             Box b = (c.y & 0x80000000) ? prim_box[leaf_prim[c.y & 0x7fffffff]] : ldcg_box(&node_box[c.y]);
+            uint32_t ma = (c.x & 0x80000000) ? leaf_prim[c.x & 0x7fffffff] : __ldcg(&node_max[c.x]);
+            uint32_t mb = (c.y & 0x80000000) ? leaf_prim[c.y & 0x7fffffff] : __ldcg(&node_max[c.y]);
             node_box[node] = box_union(a, b);
+            node_max[node] = max(ma, mb);
             node = parent[node];
         }
     }
@@ -210,6 +213,7 @@ int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaSt
     morton_tmp.reserve(m);
     bounds.reserve(6);
     node_box.reserve(m > 1 ? m - 1 : 1);
+    node_max.reserve(m > 1 ? m - 1 : 1);
     child.reserve(m > 1 ? m - 1 : 1);
     parent.reserve(2 * m);
     visits.reserve(m);
@@ -229,10 +233,44 @@ int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaSt
         k_karras<<<grid_for(m - 1, 256), 256, 0, s>>>(morton.ptr, (int)m, child.ptr, parent.ptr);
         CC_CUDA(cudaMemsetAsync(visits.ptr, 0, (m - 1) * sizeof(unsigned), s));
         k_lbvh_boxes<<<grid_for(m, 256), 256, 0, s>>>(prim_box, leaf_prim.ptr, (int)m, child.ptr, parent.ptr,
-                                                      visits.ptr, node_box.ptr);
+                                                      visits.ptr, node_box.ptr, node_max.ptr);
     }
     CC_CUDA(cudaGetLastError());
     return m > 1 ? 5 : 3;
+}
+
+// Stack traversal over the primitives with id > `above` only: subtrees whose
+// largest primitive id is <= above are skipped unvisited (self-pair queries
+// that keep the canonical order e < f). Otherwise as lbvh_traverse.
+template <class NodeOk, class LeafOk, class Visit>
+__device__ __forceinline__ bool lbvh_traverse_above(const LbvhView& t, uint32_t above, NodeOk node_ok, LeafOk leaf_ok,
+                                                    Visit visit) {
+    if (t.m == 0) return true;
+    if (t.m == 1) {
+        uint32_t p = t.leaf_prim[0];
+        if (p > above && leaf_ok(t.prim_box[p])) visit(p);
+        return true;
+    }
+    int stack[96];
+    int sp = 0;
+    if (t.node_max[0] <= above || !node_ok(t.node_box[0])) return true;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        int node = stack[--sp];
+        int2 c = t.child[node];
+        int cs[2] = {c.x, c.y};
+        for (int k = 0; k < 2; ++k) {
+            int ch = cs[k];
+            if (ch & 0x80000000) {
+                uint32_t p = t.leaf_prim[ch & 0x7fffffff];
+                if (p > above && leaf_ok(t.prim_box[p])) visit(p);
+            } else if (t.node_max[ch] > above && node_ok(t.node_box[ch])) {
+                if (sp >= 96) return false;
+                stack[sp++] = ch;
+            }
+        }
+    }
+    return true;
 }
 
 // Stack traversal. node_ok(box) prunes internal nodes; leaf_ok(box) is the
@@ -517,7 +555,7 @@ __global__ void k_ee_query(WorldView w, const uint32_t* edge_moving, uint32_t n_
             unsigned long long i = atomicAdd(count, 1ull);
             if (i < cap) out[i] = make_uint2(e, f);
         };
-        bool ok = lbvh_traverse(edge_moving_t, node_ok, leaf_ok, visit_moving);
+        bool ok = lbvh_traverse_above(edge_moving_t, e, node_ok, leaf_ok, visit_moving);
         ok = lbvh_traverse(edge_fixed_t, node_ok, leaf_ok, visit_fixed) && ok;
         if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
     }

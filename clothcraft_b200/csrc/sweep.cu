@@ -78,10 +78,8 @@ __device__ __forceinline__ d3 pos(const SweepView& s, uint32_t i, uint32_t v, d3
 // membrane (src/energy.rs:17-29) of triangle t with vertex slot `slot` at p.
 // D: derivatives; HS: also the Hessian (a gradient-only evaluation skips it)
 template <bool D, bool HS = D>
-__device__ __forceinline__ double membrane_term(const SweepView& s, uint32_t t, uint32_t slot, d3 p, d3& g, Sym& H) {
-    int4 tv = s.tri_v[t];
-    double4 cf = s.tri_coef[t];
-    double A = s.tri_area[t];
+__device__ __forceinline__ double membrane_rec(const SweepView& s, int4 tv, double4 cf, double A, uint32_t slot, d3 p,
+                                               d3& g, Sym& H) {
     MatParams M = s.mats[tv.w];
     d3 x0 = slot == 0 ? p : ld3(s.x, (uint32_t)tv.x);
     d3 x1 = slot == 1 ? p : ld3(s.x, (uint32_t)tv.y);
@@ -108,6 +106,11 @@ __device__ __forceinline__ double membrane_term(const SweepView& s, uint32_t t, 
     return A * (fw + fv + 0.5 * M.shear * sh * sh);
 }
 
+template <bool D, bool HS = D>
+__device__ __forceinline__ double membrane_term(const SweepView& s, uint32_t t, uint32_t slot, d3 p, d3& g, Sym& H) {
+    return membrane_rec<D, HS>(s, s.tri_v[t], s.tri_coef[t], s.tri_area[t], slot, p, g, H);
+}
+
 // P_k [a]x / l as three columns: P(a x e_j)/l, P y = y - h (h.y)
 __device__ __forceinline__ void proj_skew_cols(d3 a, d3 h, double inv_l, double sign, d3& c0, d3& c1, d3& c2) {
     d3 e0 = mk(0.0, a.z, -a.y), e1 = mk(-a.z, 0.0, a.x), e2 = mk(a.y, -a.x, 0.0);
@@ -132,9 +135,8 @@ __device__ __forceinline__ void add_curvature(Sym& Hm, d3 a, d3 h, d3 d, double 
 // bending (src/energy.rs:31-46) of hinge h with vertex slot `slot` at p.
 // n1 = e x u, n2 = w x e are affine in one vertex: dn_k/dp = [a_k]x.
 template <bool D, bool HS = D>
-__device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, uint32_t slot, d3 p, d3& g, Sym& H) {
-    uint4 hv = s.hinge_v[hi];
-    double K = s.hinge_k[hi];
+__device__ __forceinline__ double bending_rec(const SweepView& s, uint4 hv, double K, uint32_t slot, d3 p, d3& g,
+                                              Sym& H) {
     d3 x0 = slot == 0 ? p : ld3(s.x, hv.x);
     d3 x1 = slot == 1 ? p : ld3(s.x, hv.y);
     d3 x2 = slot == 2 ? p : ld3(s.x, hv.z);
@@ -172,6 +174,11 @@ __device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, 
 #pragma unroll
     for (int k = 0; k < 6; ++k) H.a[k] += f * Hm.a[k];
     return energy;
+}
+
+template <bool D, bool HS = D>
+__device__ __forceinline__ double bending_term(const SweepView& s, uint32_t hi, uint32_t slot, d3 p, d3& g, Sym& H) {
+    return bending_rec<D, HS>(s, s.hinge_v[hi], s.hinge_k[hi], slot, p, g, H);
 }
 
 // stitch 0.5 k |sum w_j x_j|^2 (src/vbd.rs:217-227)
@@ -504,13 +511,65 @@ __device__ __forceinline__ double local_part(const SweepView& s, uint32_t v, d3 
     // entries are grouped by type: one lane-strided loop per type, no per-entry dispatch
     uint32_t b0 = s.inc_off[v], b1 = s.inc_off[v + 1];
     uint2 mid = s.inc_mid[v];
-    for (uint32_t k = b0 + lane; k < mid.x; k += G) {
-        uint32_t ent = s.inc[k];
-        e += membrane_term<D, HS>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
+    // each loop loads the next term's record before it evaluates the current one
+    {
+        uint32_t k = b0 + lane;
+        uint32_t ent = k < mid.x ? s.inc[k] : 0u;
+        int4 tv = make_int4(0, 0, 0, 0);
+        double4 cf = make_double4(0, 0, 0, 0);
+        double A = 0.0;
+        if (k < mid.x) {
+            uint32_t t = ent & 0x0fffffffu;
+            tv = s.tri_v[t];
+            cf = s.tri_coef[t];
+            A = s.tri_area[t];
+        }
+        for (; k < mid.x; k += G) {
+            uint32_t kn = k + G;
+            uint32_t en = 0u;
+            int4 tvn = tv;
+            double4 cfn = cf;
+            double An = A;
+            if (kn < mid.x) {
+                en = s.inc[kn];
+                uint32_t t = en & 0x0fffffffu;
+                tvn = s.tri_v[t];
+                cfn = s.tri_coef[t];
+                An = s.tri_area[t];
+            }
+            e += membrane_rec<D, HS>(s, tv, cf, A, (ent >> 28) & 3u, p, g, H);
+            ent = en;
+            tv = tvn;
+            cf = cfn;
+            A = An;
+        }
     }
-    for (uint32_t k = mid.x + lane; k < mid.y; k += G) {
-        uint32_t ent = s.inc[k];
-        e += bending_term<D, HS>(s, ent & 0x0fffffffu, (ent >> 28) & 3u, p, g, H);
+    {
+        uint32_t k = mid.x + lane;
+        uint32_t ent = k < mid.y ? s.inc[k] : 0u;
+        uint4 hv = make_uint4(0, 0, 0, 0);
+        double K = 0.0;
+        if (k < mid.y) {
+            uint32_t h = ent & 0x0fffffffu;
+            hv = s.hinge_v[h];
+            K = s.hinge_k[h];
+        }
+        for (; k < mid.y; k += G) {
+            uint32_t kn = k + G;
+            uint32_t en = 0u;
+            uint4 hvn = hv;
+            double Kn = K;
+            if (kn < mid.y) {
+                en = s.inc[kn];
+                uint32_t h = en & 0x0fffffffu;
+                hvn = s.hinge_v[h];
+                Kn = s.hinge_k[h];
+            }
+            e += bending_rec<D, HS>(s, hv, K, (ent >> 28) & 3u, p, g, H);
+            ent = en;
+            hv = hvn;
+            K = Kn;
+        }
     }
     for (uint32_t k = mid.y + lane; k < b1; k += G) e += stitch_term<D>(s, s.inc[k] & 0x0fffffffu, v, p, g, H);
     uint32_t c1 = s.contacts.inc_off[v + 1];

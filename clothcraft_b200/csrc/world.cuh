@@ -20,11 +20,13 @@ struct LbvhView {
     const int2* child;        // [m-1] children; bit 31 set = leaf (sorted position)
     const uint32_t* leaf_prim;  // [m] primitive id of each sorted leaf
     const Box* prim_box;      // global primitive boxes, indexed by primitive id
+    const uint32_t* node_max;  // [m-1] largest primitive id under each internal node
 };
 
 struct Lbvh {
     uint32_t m = 0;
     DBuf<Box> node_box;
+    DBuf<uint32_t> node_max;
     DBuf<int2> child;
     DBuf<int> parent;       // [2m-1]: internal 0..m-2, leaves m-1..2m-2
     DBuf<unsigned> visits;  // [m-1]
@@ -36,7 +38,7 @@ struct Lbvh {
     // returns the number of this library's kernels launched
     int build(const Box* prim_box, const uint32_t* ids, uint32_t m, cudaStream_t s);
     LbvhView view(const Box* prim_box) const {
-        return {m, node_box.ptr, child.ptr, leaf_prim.ptr, prim_box};
+        return {m, node_box.ptr, child.ptr, leaf_prim.ptr, prim_box, node_max.ptr};
     }
 };
 
