@@ -465,7 +465,8 @@ def main():
         "e2e": {"value": world * K / (t_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 2 * sc.n * 32,
                 "d2h_bytes_per_step": 2 * sc.n * 32},
         "gpu_launches": int(sum(m["kernel_launches"] for m in mets_l)),
-        "lanes_per_vertex": int(L.cc_solver_get_lanes(learned.h)),
+        "lanes_per_vertex": int(L.cc_solver_get_lanes(learned.h)) & 0xff,
+        "blocks_per_sm_cap": int(L.cc_solver_get_lanes(learned.h)) >> 8,
         "breakdown_ms_per_step": {
             "detection": sum(m["detection_ms"] for m in mets_l) / K,
             "coloring": sum(m["color_ms"] for m in mets_l) / K,

@@ -1187,12 +1187,16 @@ int32_t cc_solver_set_profiling(cc_solver* s, int32_t enable) {
     return CC_OK;
 }
 int32_t cc_solver_set_lanes(cc_solver* s, int32_t lanes) {
-    if (!(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32))
-        return s->fail(Failure{CC_ERR_INVALID_ARGUMENT, "lanes must be 0 (autotune) or a power of two up to 32"});
-    s->lanes = lanes == 0 ? 0 : (lanes | 3 << 8);
+    int32_t g = lanes & 0xff, cap = lanes >> 8;
+    if (!(g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) || cap < 0 || cap > 5 ||
+        (g == 0 && cap != 0) || (cap != 0 && cap < 3))
+        return s->fail(Failure{CC_ERR_INVALID_ARGUMENT,
+                               "lanes must be 0 (autotune) or a power of two up to 32, optionally | cap << 8 with "
+                               "cap in 3..5"});
+    s->lanes = lanes == 0 ? 0 : (g | (cap ? cap : 3) << 8);
     return CC_OK;
 }
-int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes & 0xff; }
+int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes; }
 cc_world* cc_solver_world(cc_solver* s) { return &s->world_view; }
 
 static void upload_state(cc_solver* s, const double* x, const double* v) {
