@@ -7,7 +7,8 @@
 than the benchmark's seed 1). Each variant runs `warm` plain steps into its
 fold phase, then `steps` sampled steps solved to a tight residual target.
 `garment`: seeded variants of the sewn garment proxy (config3), sampled from
-the start. Samples stay in HBM (features float32 [rows, 24], targets
+the start. `crumple`: seeded 1024x1024 crumple sheets (config4) with their
+corners driven inward between steps. Samples stay in HBM (features float32 [rows, 24], targets
 float32 [rows, 3]); the network trains with the library's own FP32
 forward/backward and Adam kernels (cc_mlp_train) and is saved as .npz.
 Needs a CUDA device; there is no CPU path.
@@ -46,6 +47,10 @@ def _make_fold(seed):
     return scenes.config1(seed=seed)
 
 
+def _make_crumple(seed):
+    return scenes.config4(seed=seed)
+
+
 def build_scenes(factory, seeds, workers: int = 0):
     """Scene generation is CPU work (Poisson-disk sampling for garments):
     spread it over a spawn-started process pool."""
@@ -57,8 +62,16 @@ def build_scenes(factory, seeds, workers: int = 0):
         return pool.map(factory, seeds)
 
 
+def _drive(sc, solver):
+    """Driven-corner kinematics of the crumple scene: move the pinned rows of
+    the resident state to the next step's positions (breaks the adaptive-guess
+    history, as the reference's callers do)."""
+    x, v, t = solver.get_state()
+    solver.set_state(scenes.driven_corners(sc, x, t + sc.settings.dt), v, t)
+
+
 def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, cap: int = 200, check: int = 2,
-             log=print):
+             log=print, driven: bool = False):
     """Plain vs learned init at a residual target on each scene: `warm` plain
     steps, then `steps` steps per init from the same state. Returns a list of
     per-scene dicts (mean iterations, device ms per step, learned-used fraction)."""
@@ -67,6 +80,8 @@ def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, ca
         g = VbdSolver(sc)
         g.set_state(sc.x0, sc.v0, 0.0)
         for _ in range(warm):
+            if driven:
+                _drive(sc, g)
             g.step_resident(sc.settings.to_c())
         start = g.get_state()
         row = {"scene": sc.name + ":" + sc.note}
@@ -78,6 +93,8 @@ def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, ca
             st = sample_settings(sc, tolerance, cap, check, mode)
             its, ms, used = [], [], []
             for _ in range(steps):
+                if driven:
+                    _drive(sc, h)
                 m = h.step_resident(st)
                 its.append(m["iterations"])
                 ms.append(m["gpu_compute_ms"])
@@ -95,7 +112,7 @@ def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, ca
 
 
 def collect(scene_list, warm: int, steps: int, tolerance: float = 1e-4, cap: int = 200, check: int = 5,
-            log=print):
+            log=print, driven: bool = False):
     """Run each scene `warm` plain steps, then `steps` sampled steps; returns
     (features, targets) CUDA tensors with one row per free vertex and step."""
     import torch
@@ -106,6 +123,8 @@ def collect(scene_list, warm: int, steps: int, tolerance: float = 1e-4, cap: int
         g = VbdSolver(sc)
         g.set_state(sc.x0, sc.v0, 0.0)
         for _ in range(warm):
+            if driven:
+                _drive(sc, g)
             g.step_resident(sc.settings.to_c())
         rows = g.free_vertices
         F = torch.empty((steps * rows, 24), dtype=torch.float32, device="cuda")
@@ -113,6 +132,8 @@ def collect(scene_list, warm: int, steps: int, tolerance: float = 1e-4, cap: int
         st = sample_settings(sc, tolerance, cap, check)
         its = []
         for k in range(steps):
+            if driven:
+                _drive(sc, g)
             m = g.step_sample(st, F[k * rows:(k + 1) * rows], T[k * rows:(k + 1) * rows])
             its.append(m["iterations"])
         feats.append(F)
@@ -140,9 +161,13 @@ def garment_scenes(variants: int, first_seed: int = 100, workers: int = 0):
     return build_scenes(_make_garment, [first_seed + k for k in range(variants)], workers)
 
 
+def crumple_scenes(variants: int, first_seed: int = 200, workers: int = 0):
+    return build_scenes(_make_crumple, [first_seed + k for k in range(variants)], workers)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("kind", choices=["fold", "garment"])
+    ap.add_argument("kind", choices=["fold", "garment", "crumple"])
     ap.add_argument("--out", default=None)
     ap.add_argument("--variants", type=int, default=None)
     ap.add_argument("--warm", type=int, default=None)
@@ -161,11 +186,14 @@ def main(argv=None):
         if args.kind == "fold":
             scs = fold_scenes(args.variants or 6, workers=args.workers)
             warm, steps = (args.warm if args.warm is not None else 190), (args.steps or 40)
-        else:
+        elif args.kind == "garment":
             scs = garment_scenes(args.variants or 50, workers=args.workers)
             warm, steps = (args.warm if args.warm is not None else 0), (args.steps or 100)
+        else:
+            scs = crumple_scenes(args.variants or 2, workers=args.workers)
+            warm, steps = (args.warm if args.warm is not None else 20), (args.steps or 20)
         print("collecting %d variants" % len(scs), flush=True)
-        F, T = collect(scs, warm, steps, tolerance=args.tolerance)
+        F, T = collect(scs, warm, steps, tolerance=args.tolerance, driven=args.kind == "crumple")
         net, losses = train(F, T, steps=args.train_steps)
         del F, T
         os.makedirs(os.path.dirname(out), exist_ok=True)
@@ -175,11 +203,14 @@ def main(argv=None):
         if args.kind == "fold":
             held = fold_scenes(args.evaluate, first_seed=1000, workers=args.workers)
             warm = 200
-        else:
+        elif args.kind == "garment":
             held = garment_scenes(args.evaluate, first_seed=10000, workers=args.workers)
             warm = 10
+        else:
+            held = crumple_scenes(args.evaluate, first_seed=20000, workers=args.workers)
+            warm = 30
         print("evaluating on %d held-out seeds (tolerance 1e-3)" % len(held), flush=True)
-        rows = evaluate(net, held, warm, args.eval_steps)
+        rows = evaluate(net, held, warm, args.eval_steps, driven=args.kind == "crumple")
         tr = [r["time_ratio"] for r in rows]
         ir = [r["iteration_ratio"] for r in rows]
         print("held-out summary: time ratio plain/learned mean %.3f median %.3f; iteration ratio mean %.3f median %.3f"
