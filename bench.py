@@ -13,9 +13,12 @@ generator), then runs W warm-up and K timed steps.
 Equal residual: every step iterates until the relative force residual
 ||P grad E(x)|| / ||grad E(y)|| <= 1e-3 (evaluated every 2 iterations, at most
 200 iterations, the reference's limit). `value` is the learned-init form
-(MLP correction of the adaptive guess, energy-checked); the plain adaptive
-init runs alongside (`plain`), and so does the reference's fixed 30-iteration
-step (`fixed_iterations`). The network is clothcraft_b200/data/fold_init_mlp.npz,
+(MLP correction of the adaptive guess, energy-checked) with Chebyshev
+acceleration of the sweeps (rho 0.95, restarted when a residual evaluation
+rises); the plain adaptive init runs alongside with the same acceleration
+(`plain`), both inits run without it (`unaccelerated`, the reference's
+iteration), and so does the reference's fixed 30-iteration step
+(`fixed_iterations`). The network is clothcraft_b200/data/fold_init_mlp.npz,
 trained by `python -m clothcraft_b200.train_init fold` on other seeds.
 
   python bench.py [--gpus N --steps K --warmup W]      # B200 library
@@ -47,6 +50,7 @@ CHECK_EVERY = 2
 ITERATION_CAP = 200
 FIXED_ITERATIONS = 30
 STALL_REFRESH = 2  # refresh the OGC balls after 2 checks without a 5 % residual decrease
+ACCELERATION = 0.95  # Chebyshev spectral-radius estimate of the equal-residual legs
 MLP_PATH = os.path.join(ROOT, "clothcraft_b200", "data", "fold_init_mlp.npz")
 UNIT = "steps/s"
 L2_FLUSH_BYTES = 256 << 20
@@ -189,16 +193,19 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def step_settings(sc, mode, iterations=None):
-    """Equal-residual settings (mode 0 adaptive, 1 learned), or a fixed
-    iteration count with no residual target when `iterations` is given."""
+def step_settings(sc, mode, iterations=None, acceleration=ACCELERATION):
+    """Equal-residual settings (mode 0 adaptive, 1 learned) with the given
+    Chebyshev acceleration, or a fixed iteration count with neither a
+    residual target nor acceleration when `iterations` is given."""
     s = sc.settings
     if iterations is None:
         s.iterations, s.residual_tolerance, s.residual_check_every = ITERATION_CAP, TOLERANCE, CHECK_EVERY
         s.stall_refresh = STALL_REFRESH
+        s.acceleration = acceleration
     else:
         s.iterations, s.residual_tolerance, s.residual_check_every = iterations, 0.0, 0
         s.stall_refresh = 0
+        s.acceleration = 0.0
     s.init_mode = mode
     return s.to_c()
 
@@ -211,7 +218,7 @@ def cpu_reference_run(sc, state, steps, budget_s, threads, warmup=0):
     import oracle
 
     o = oracle.Solver(sc, threads=threads)
-    st = step_settings(sc, 0)
+    st = step_settings(sc, 0, acceleration=0.0)  # the reference's iteration and init
     x, v, t = state
     t0 = time.perf_counter()
     warm = 0
@@ -302,7 +309,7 @@ def main():
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     start = fold_state()
 
-    def make(mode, iterations=None):
+    def make(mode, iterations=None, acceleration=ACCELERATION):
         s = VbdSolver(sc)
         if args.lanes and L.cc_solver_set_lanes(s.h, args.lanes) != 0:
             raise SystemExit("invalid --lanes %d" % args.lanes)
@@ -310,7 +317,7 @@ def main():
             s.set_mlp(net, 1)
         s.set_state(*start)
         for _ in range(args.warmup):
-            s.step_resident(step_settings(sc, mode, iterations))
+            s.step_resident(step_settings(sc, mode, iterations, acceleration))
         return s
 
     def timed(solver, step_fn, k):
@@ -354,6 +361,12 @@ def main():
     t_l, mets_l = leg(learned, lambda: learned.step_resident(st_l), K)
     # ---- plain adaptive init at equal residual
     t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
+    # ---- both inits without acceleration (the reference's iteration)
+    unacc = {}
+    for mode in (0, 1):
+        su = step_settings(sc, mode, acceleration=0.0)
+        solver_u = make(mode, acceleration=0.0)
+        unacc[mode] = leg(solver_u, lambda: solver_u.step_resident(su), K)
     # ---- end to end through cc_solver_step with host arrays (learned)
     e2e_solver = make(1)
     x, v, t = e2e_solver.get_state()
@@ -378,7 +391,7 @@ def main():
     # steps stop early once converged; both inits
     budget = {}
     for mode in (0, 1):
-        sb = step_settings(sc, mode)
+        sb = step_settings(sc, mode, acceleration=0.0)
         sb.iterations = FIXED_ITERATIONS
         solver_b = make(mode, FIXED_ITERATIONS)
         budget[mode] = leg(solver_b, lambda: solver_b.step_resident(sb), K)
@@ -396,7 +409,8 @@ def main():
                 "vertex_iters_per_s": world * free * sum(its) / (t_ms / 1000.0),
                 "mean_iterations": float(np.mean(its)), "median_iterations": float(np.median(its)),
                 "capped_fraction": float(np.mean(np.array(its) >= ITERATION_CAP)),
-                "mean_final_relative_residual": float(np.mean([m["relative_residual"] for m in mets]))}
+                "mean_final_relative_residual": float(np.mean([m["relative_residual"] for m in mets])),
+                "max_final_relative_residual": float(np.max([m["relative_residual"] for m in mets]))}
 
     # ---- roofline of the dominant kernel (colour sweep), learned leg
     peak, peak_kind = load_peaks()
@@ -438,6 +452,10 @@ def main():
         "plain": summary(t_p, mets_p),
         "learned_vs_plain_time_ratio": t_p / t_l,
         "learned_init_used_fraction": float(np.mean([m["init_used"] for m in mets_l])),
+        "acceleration": ACCELERATION,
+        "unaccelerated": {"learned": summary(*unacc[1]), "plain": summary(*unacc[0]),
+                          "learned_vs_plain_time_ratio": unacc[0][0] / unacc[1][0],
+                          "note": "same residual target, Chebyshev acceleration off (the reference's iteration)"},
         "fixed_iterations": {"iterations": FIXED_ITERATIONS, "steps_per_s": world * K / (t_f / 1000.0),
                              "ms_per_step": t_f / K,
                              "mean_final_relative_residual": float(np.mean([m["relative_residual"]

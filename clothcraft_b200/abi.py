@@ -83,6 +83,7 @@ class cc_vbd_settings(C.Structure):
         ("residual_tolerance", C.c_double),
         ("residual_check_every", C.c_uint32),
         ("stall_refresh", C.c_uint32),
+        ("acceleration", C.c_double),
     ]
 
 

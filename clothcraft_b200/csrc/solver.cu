@@ -52,7 +52,8 @@ bool ogc_valid(const cc_ogc_settings& s) {  // src/ogc/world.rs:56-70
 bool vbd_valid(const cc_vbd_settings& s) {  // src/vbd.rs:38-51
     return ogc_valid(s.contact) && std::isfinite(s.dt) && s.dt >= 1e-6 && s.dt <= 0.025 && s.iterations != 0 &&
            s.iterations <= 200 && std::isfinite(s.damping) && s.damping >= 0.0 && std::isfinite(s.gravity[0]) &&
-           std::isfinite(s.gravity[1]) && std::isfinite(s.gravity[2]);
+           std::isfinite(s.gravity[1]) && std::isfinite(s.gravity[2]) && std::isfinite(s.acceleration) &&
+           s.acceleration >= 0.0 && s.acceleration < 1.0;
 }
 }  // namespace
 
@@ -65,6 +66,9 @@ struct StepScalars {
     unsigned int error;
     unsigned int mismatch;
     unsigned int clipped;
+    unsigned int acc_k;         // Chebyshev: iterations since the sequence's (re)start
+    double acc_w;               // Chebyshev weight of the current iteration
+    double acc_g2;              // Chebyshev: residual of the previous evaluation
     unsigned int refresh_at;    // first iteration whose start needs a refresh detection
     unsigned int converged_at;  // iterations run when the residual target was met
     unsigned int stop_at;       // min(refresh_at, converged_at): later sweeps exit at once
@@ -137,6 +141,32 @@ __global__ void k_copy_positions(uint32_t n, const double4* src, double4* dst) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
 }
 
+// Chebyshev step after iteration `it` (no reference counterpart):
+// x = w (x_sweep - x_prev2) + x_prev2 on free vertices, clipped to the OGC
+// ball, from the second iteration of a sequence on (acc_k >= 2); `hist`
+// holds x_prev2 on entry and the new x on exit (it becomes the previous
+// iterate of the next call).
+__global__ void k_accelerate(uint32_t n, const uint8_t* pinned, ContactsView c, double4* x, double4* hist,
+                             const StepScalars* sc, uint32_t it) {
+    if (sc->stop_at <= it) return;  // this iteration was skipped
+    const bool extrapolate = sc->acc_k >= 2;
+    const double w = sc->acc_w;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        d3 p = ld3(x, i);
+        if (extrapolate && !pinned[i]) {
+            d3 q = ld3(hist, i);
+            p = mk(__fma_rn(w, p.x - q.x, q.x), __fma_rn(w, p.y - q.y, q.y), __fma_rn(w, p.z - q.z, q.z));
+            d3 ctr = ld3(c.centers, i);
+            d3 d = p - ctr;
+            double l = len(d);
+            double b = c.radii[i];
+            if (l > b) p = ctr + d * (b / l);
+            st3(x, i, p);
+        }
+        st3(hist, i, p);
+    }
+}
+
 // Conservative warm start (src/vbd.rs:316-324)
 __global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* guess, ContactsView c, double4* x,
                              unsigned int* clipped) {
@@ -161,8 +191,19 @@ __global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* g
 // Refresh rule after iteration `it` (src/vbd.rs:326): the next iteration
 // starts with a new detection when at least refresh_fraction * n vertices
 // were clipped. Later sweeps already enqueued see refresh_at and skip.
-__global__ void k_refresh_rule(StepScalars* sc, uint32_t it, uint32_t iterations, double threshold) {
+// With acceleration (rho2 = rho^2 > 0) it also advances the Chebyshev
+// sequence (Wang 2015, "A Chebyshev semi-iterative approach for accelerating
+// projective and position-based dynamics"): w1 = 1, w2 = 2/(2 - rho^2),
+// wk = 4/(4 - rho^2 w(k-1)), rounded operation by operation as on the CPU.
+__global__ void k_refresh_rule(StepScalars* sc, uint32_t it, uint32_t iterations, double threshold, double rho2) {
     if (sc->stop_at <= it) return;  // this iteration was skipped
+    if (rho2 > 0.0) {
+        unsigned int k = ++sc->acc_k;
+        double w = 1.0;
+        if (k == 2) w = __ddiv_rn(2.0, __dsub_rn(2.0, rho2));
+        else if (k > 2) w = __ddiv_rn(4.0, __dsub_rn(4.0, __dmul_rn(rho2, sc->acc_w)));
+        sc->acc_w = w;
+    }
     unsigned int c = sc->clipped_iter[it];
     if (c > 0 && (double)c >= threshold && it + 1 < iterations) {
         sc->refresh_at = it + 1;
@@ -177,14 +218,21 @@ __global__ void k_refresh_rule(StepScalars* sc, uint32_t it, uint32_t iterations
 // With `stall` = k > 0, k evaluations in a row without a 5 % decrease of the
 // residual, while vertices are being clipped, request a refresh detection
 // before the next iteration (new OGC balls around the current positions).
+// With acceleration, an evaluation above the previous one restarts the
+// Chebyshev sequence (the next iteration is a plain sweep again).
 __global__ void __launch_bounds__(256) k_residual_rule(StepScalars* sc, const double* partial, uint32_t it,
-                                                       uint32_t iterations, double tol2, int stop, uint32_t stall) {
+                                                       uint32_t iterations, double tol2, int stop, uint32_t stall,
+                                                       int accelerate) {
     if (sc->stop_at <= it) return;  // uniform: every thread reads it before thread 0 writes
     double g2 = block_sum_partials(partial);
     if (threadIdx.x == 0) {
         sc->gx2 = g2;
         sc->gx2_iter[it] = g2;
         sc->checked_at = it + 1;
+        if (accelerate) {
+            if (g2 > sc->acc_g2) sc->acc_k = 0;
+            sc->acc_g2 = g2;
+        }
         if (stop && g2 <= tol2 * sc->gy2 && sc->converged_at > it + 1) {
             sc->converged_at = it + 1;
             if (it + 1 < iterations) sc->stop_at = min(sc->stop_at, it + 1);
@@ -387,6 +435,7 @@ struct cc_solver {
     double mean_mass = 1.0;
     DBuf<float> feat, corr;
     DBuf<double4> best, prev_corr;
+    DBuf<double4> acc_a, acc_b;  // Chebyshev history: the last two iterates
     bool step_history = false;  // the adaptive-guess history test of the current step (host part)
     float* sample_features = nullptr;  // caller device buffers of cc_solver_step_sample
     float* sample_targets = nullptr;
@@ -705,6 +754,12 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     const double threshold = s.contact.refresh_fraction * (double)n;
     const double tol2 = s.residual_tolerance * s.residual_tolerance;
     const bool target_on = s.residual_tolerance > 0.0;
+    const bool accelerate = s.acceleration > 0.0;
+    const double rho2 = accelerate ? s.acceleration * s.acceleration : 0.0;
+    if (accelerate) {
+        acc_a.reserve(n);
+        acc_b.reserve(n);
+    }
     bool need_refresh = clipped > 0 && (double)clipped >= threshold;
     std::vector<std::pair<size_t, uint32_t>> prof_pairs;  // (event index, iteration)
     std::vector<uint32_t> prof_ok;
@@ -720,6 +775,14 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         SweepView sv = sweep_view(cv, s, grab);
         sv.skip_at = &sc.ptr->stop_at;
         if (lanes == 0) autotune(sv);
+        // the Chebyshev sequence restarts with every batch (the step's start or a refresh)
+        double4* acc_prev1 = acc_a.ptr;
+        double4* acc_prev2 = acc_b.ptr;
+        if (accelerate) {
+            CC_CUDA(cudaMemcpyAsync(acc_prev1, world->x(), n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
+            CC_CUDA(cudaMemsetAsync(&sc.ptr->acc_k, 0, sizeof(unsigned int), stream));
+            CC_CUDA(cudaMemsetAsync(&sc.ptr->acc_g2, 0x7f, sizeof(double), stream));  // ~1.4e306
+        }
         CC_CUDA(cudaMemsetAsync(&sc.ptr->refresh_at, 0xff, 2 * sizeof(unsigned int), stream));  // + converged_at
         CC_CUDA(cudaMemsetAsync(&sc.ptr->stall_best, 0x7f, sizeof(double), stream));  // ~1.4e306
         CC_CUDA(cudaMemsetAsync(&sc.ptr->stall_count, 0, sizeof(unsigned int), stream));
@@ -753,13 +816,18 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                     }
                     ++own_launches;
                 }
-                k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold);
+                k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold, rho2);
+                if (accelerate) {
+                    k_accelerate<<<gb, 256, 0, stream>>>(n, pinned.ptr, cv, world->x(), acc_prev2, sc.ptr, it);
+                    std::swap(acc_prev1, acc_prev2);
+                    ++own_launches;
+                }
                 ++own_launches;
                 if (checks && ((it + 1) % check_every == 0 || it + 1 == s.iterations)) {
                     launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, lanes, true, stream);
                     launch_sum_partial(gsq.ptr, n, partial.ptr, &sc.ptr->stop_at, it, stream);
                     k_residual_rule<<<1, 256, 0, stream>>>(sc.ptr, partial.ptr, it, s.iterations, tol2,
-                                                           target_on ? 1 : 0, s.stall_refresh);
+                                                           target_on ? 1 : 0, s.stall_refresh, accelerate ? 1 : 0);
                     own_launches += 3;
                 }
             }

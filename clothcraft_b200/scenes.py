@@ -356,6 +356,7 @@ class StepSettings:
     residual_tolerance: float = 0.0
     residual_check_every: int = 0
     stall_refresh: int = 0
+    acceleration: float = 0.0  # Chebyshev rho; 0 = off (the reference)
 
     def to_c(self) -> abi.cc_vbd_settings:
         s = abi.cc_vbd_settings()
@@ -365,6 +366,7 @@ class StepSettings:
         s.residual_tolerance = self.residual_tolerance
         s.residual_check_every = self.residual_check_every
         s.stall_refresh = self.stall_refresh
+        s.acceleration = self.acceleration
         s.damping = self.damping
         for k in range(3):
             s.gravity[k] = self.gravity[k]

@@ -132,6 +132,7 @@ typedef struct cc_vbd_settings {
     double residual_tolerance;       /* 0 = run all `iterations`            */
     uint32_t residual_check_every;   /* 0 = no relative residual            */
     uint32_t stall_refresh;          /* 0 = off                             */
+    double acceleration;             /* Chebyshev rho in [0, 1); 0 = off     */
 } cc_vbd_settings;
 
 /* Grab (src/vbd.rs:54-60): mouse attachment, weights sum to one. */

@@ -57,6 +57,7 @@ VbdSettings to_vbd(const cc_vbd_settings* s) {
     o.residual_tolerance = s->residual_tolerance;
     o.residual_check_every = s->residual_check_every;
     o.stall_refresh = s->stall_refresh;
+    o.acceleration = s->acceleration;
     return o;
 }
 

@@ -15,7 +15,18 @@ static double now_ms() {
 bool VbdSettings::valid() const {  // src/vbd.rs:38-51
     if (!contact.valid()) return false;
     return std::isfinite(dt) && dt >= 1e-6 && dt <= 0.025 && iterations != 0 && iterations <= 200 &&
-           std::isfinite(damping) && damping >= 0.0 && finite(gravity);
+           std::isfinite(damping) && damping >= 0.0 && finite(gravity) && std::isfinite(acceleration) &&
+           acceleration >= 0.0 && acceleration < 1.0;
+}
+
+// Chebyshev weight of the k-th iteration since the last (re)start
+// (Wang 2015, "A Chebyshev semi-iterative approach for accelerating
+// projective and position-based dynamics"): w1 = 1, w2 = 2/(2 - rho^2),
+// wk = 4/(4 - rho^2 w(k-1)).
+double chebyshev_omega(size_t k, double rho) {
+    double r2 = rho * rho, w = 1.0;
+    for (size_t j = 2; j <= k; ++j) w = j == 2 ? 2.0 / (2.0 - r2) : 4.0 / (4.0 - r2 * w);
+    return w;
 }
 
 // src/vbd/prediction.rs:15-41
@@ -287,6 +298,15 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
         metrics.has_relative_residual = true;
     }
     std::vector<Update> updates;
+    // Chebyshev acceleration: x(k) = w_k (sweep result - x(k-2)) + x(k-2),
+    // clipped to the OGC ball, from the second iteration after each
+    // (re)start; a refresh detection, and a residual evaluation above the
+    // previous one, restart the sequence.
+    const bool accelerate = settings.acceleration > 0.0;
+    std::vector<D3> acc_prev1, acc_prev2;
+    size_t acc_k = 0;
+    double acc_g2 = HUGE_VAL;
+    if (accelerate) acc_prev1 = x;
     double stall_best = HUGE_VAL;
     size_t stall_count = 0;
     bool stall_pending = false;
@@ -302,6 +322,11 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
             metrics.detection_updates += 1;
             metrics.broad_phase_rebuilds += contacts.broad_phase_rebuilt ? 1 : 0;
             add_profile(contacts.profile);
+            if (accelerate) {
+                acc_k = 0;
+                acc_g2 = HUGE_VAL;
+                acc_prev1 = x;
+            }
         }
         clipped = 0;
         double residual = 0.0;
@@ -355,6 +380,21 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
                 residual += u.residual;
             }
         }
+        if (accelerate) {
+            double w = chebyshev_omega(++acc_k, settings.acceleration);
+            if (acc_k >= 2) {
+                for (size_t v = 0; v < n; ++v) {
+                    if (mesh.pinned[v]) continue;
+                    const D3& p = acc_prev2[v];
+                    D3 q{std::fma(w, x[v].x - p.x, p.x), std::fma(w, x[v].y - p.y, p.y),
+                         std::fma(w, x[v].z - p.z, p.z)};
+                    bool b;
+                    x[v] = contacts.truncate(v, q, b);
+                }
+            }
+            acc_prev2.swap(acc_prev1);
+            acc_prev1 = x;
+        }
         metrics.truncated_vertices += clipped;
         metrics.residual_rms_n = std::sqrt(residual / (double)(3 * n));
         metrics.has_residual = true;
@@ -362,6 +402,10 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
         if (checks && ((it + 1) % check_every == 0 || it + 1 == settings.iterations)) {
             double gx2 = grad_sq(x, contacts, target, inertia, settings, grab, true);
             metrics.relative_residual = std::sqrt(gx2 / gy2);
+            if (accelerate) {
+                if (gx2 > acc_g2) acc_k = 0;
+                acc_g2 = gx2;
+            }
             if (settings.residual_tolerance > 0.0 &&
                 gx2 <= settings.residual_tolerance * settings.residual_tolerance * gy2) {
                 metrics.iterations = it + 1;

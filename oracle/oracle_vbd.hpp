@@ -48,6 +48,9 @@ struct VbdSettings {  // src/vbd.rs:18-52
     double residual_tolerance = 0.0;
     size_t residual_check_every = 0;
     size_t stall_refresh = 0;  // refresh after this many evaluations without a 5 % decrease
+    // Extension: Chebyshev semi-iterative acceleration of the sweeps with
+    // spectral-radius estimate rho in [0, 1) (0 = off, the reference).
+    double acceleration = 0.0;
     bool valid() const;
 };
 

@@ -122,17 +122,20 @@ def scenes_fold_state():
     return os.path.join(os.path.dirname(__file__), "golden", "sheet256_fold_state.npz")
 
 
-@pytest.mark.parametrize("tol,stall", [(2e-2, 0), (1e-4, 0), (1e-4, 2)])
-def test_residual_target_matches_oracle(tol, stall):
+@pytest.mark.parametrize("tol,stall,rho", [(2e-2, 0, 0.0), (1e-4, 0, 0.0), (1e-4, 2, 0.0), (1e-4, 2, 0.5),
+                                          (1e-4, 2, 0.8), (2e-2, 0, 0.95), (1e-4, 2, 0.95), (1e-4, 0, 0.95)])
+def test_residual_target_matches_oracle(tol, stall, rho):
     """Same stopping iteration, refresh count and positions as the oracle's
     restatement of the residual-target rule, with and without the stall
-    refresh (FP64 both; bar (a) on positions)."""
+    refresh and the Chebyshev acceleration with its restarts (FP64 both;
+    bar (a) on positions)."""
     sc = contact_scene()
     x0, v0, t0 = advance(sc, 3)
     s = settings(sc, 60, check=2, tol=tol)
     s.stall_refresh = stall
+    s.acceleration = rho
     st = s.to_c()
-    g = VbdSolver(sc)
+    g = VbdSolver(sc).set_lanes(4)
     x, _, _, m = g.step(x0, v0, t0, st)
     o = oracle.Solver(sc, threads=8)
     xo, _, _, mo = o.step(x0, v0, t0, st)
@@ -154,3 +157,37 @@ def test_last_step_trace_records_every_evaluation():
     assert np.isnan(r[0]) and np.isnan(r[1]) and np.isfinite(r[2]) and np.isfinite(r[5]) and np.isfinite(r[8])
     assert r[8] == m["relative_residual"] or abs(r[8] - m["relative_residual"]) <= 1e-15 * r[8]
     assert int(c[:9].sum()) == m["truncated_vertices"]
+
+
+def test_acceleration_fixed_iterations_match_oracle_and_keep_the_trust_region():
+    """Chebyshev acceleration over a fixed iteration count: positions within
+    bar (a) of the oracle's for three steps, every vertex inside its OGC ball
+    (the step fails its trust-region check otherwise), and the weights act."""
+    sc = contact_scene()
+    x0, v0, t0 = advance(sc, 3)
+    s = settings(sc, 24)
+    s.acceleration = 0.9
+    st = s.to_c()
+    g = VbdSolver(sc)
+    o = oracle.Solver(sc, threads=8)
+    xg, vg, tg, xo, vo, to = x0, v0, t0, x0, v0, t0
+    for _ in range(3):
+        xg, vg, tg, mg = g.step(xg, vg, tg, st)
+        xo, vo, to, mo = o.step(xo, vo, to, st)
+        assert mg["detection_updates"] == mo["detection_updates"]
+        assert np.abs(xg - xo).max() <= 1e-5
+    plain = settings(sc, 24)
+    plain.acceleration = 0.0
+    xp, _, _, _ = VbdSolver(sc).step(x0, v0, t0, plain.to_c())
+    xa, _, _, _ = VbdSolver(sc).step(x0, v0, t0, st)
+    assert np.abs(xa - xp).max() > 0.0
+
+
+def test_acceleration_out_of_range_is_rejected():
+    sc = contact_scene()
+    g = VbdSolver(sc)
+    for rho in (1.0, -0.1, float("nan")):
+        s = settings(sc, 4)
+        s.acceleration = rho
+        with pytest.raises(Exception):
+            g.step(sc.x0, sc.v0, 0.0, s.to_c())
