@@ -1,11 +1,13 @@
 """Run a few steps of the benchmark workload for a profiler.
 
-  python -m clothcraft_b200.profile_fold [--steps 2] [--lanes 4] [--learned] [--fixed N]
+  python -m clothcraft_b200.profile_fold [--steps 2] [--lanes 4] [--learned] [--fixed N] [--acceleration RHO]
 
 The 256x256 self-contact fold from its committed fold-phase state
 (tests/golden/sheet256_fold_state.npz), stepped to the benchmark's residual
 target (1e-3, checked every 2 iterations, stall refresh 2, cap 200), or a
-fixed iteration count with --fixed. Nothing is timed here: wrap it in
+fixed iteration count with --fixed; --acceleration sets the Chebyshev
+estimate of the residual-target form (the benchmark uses 0.95). Nothing is
+timed here: wrap it in
 `ncu` to see the launches of exactly this workload.
 """
 from __future__ import annotations
@@ -28,6 +30,7 @@ def main(argv=None):
     ap.add_argument("--lanes", type=int, default=4)
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--fixed", type=int, default=0)
+    ap.add_argument("--acceleration", type=float, default=0.0)
     args = ap.parse_args(argv)
     sc = scenes.config1()
     z = np.load(FOLD_STATE)
@@ -37,6 +40,7 @@ def main(argv=None):
         s.iterations = args.fixed
     else:
         s.iterations, s.residual_tolerance, s.residual_check_every, s.stall_refresh = 200, 1e-3, 2, 2
+        s.acceleration = args.acceleration
     if args.learned:
         from .learned import Mlp
 
