@@ -562,10 +562,13 @@ __global__ void k_ee_query(WorldView w, const uint32_t* edge_moving, uint32_t n_
 }
 
 // ------------------------------------------------------------ narrow phase
+// Contact keys: hi = kind << 2nb | v0 << nb | v1, lo = v2 << nb | v3, with nb
+// bits per vertex id (2^nb >= vertex count): lexicographic (kind, v0..v3)
+// order in as few radix digits as the ids need.
 __device__ __forceinline__ void push_contact(unsigned kind, uint32_t i0, uint32_t i1, uint32_t i2, uint32_t i3,
                                              double eps, unsigned long long* hi, unsigned long long* lo,
                                              double* epsv, uint32_t* idx, unsigned long long cap,
-                                             unsigned long long* count) {
+                                             unsigned long long* count, uint32_t nb) {
     // canonical vertex order (world.rs:435-452)
     uint32_t v[4] = {i0, i1, i2, i3};
     auto sw = [&](int a, int b) {
@@ -590,8 +593,8 @@ __device__ __forceinline__ void push_contact(unsigned kind, uint32_t i0, uint32_
     }
     unsigned long long k = atomicAdd(count, 1ull);
     if (k < cap) {
-        hi[k] = ((unsigned long long)kind << 62) | ((unsigned long long)v[0] << 31) | (unsigned long long)v[1];
-        lo[k] = ((unsigned long long)v[2] << 32) | (unsigned long long)v[3];
+        hi[k] = ((unsigned long long)kind << (2 * nb)) | ((unsigned long long)v[0] << nb) | (unsigned long long)v[1];
+        lo[k] = ((unsigned long long)v[2] << nb) | (unsigned long long)v[3];
         epsv[k] = eps;
         idx[k] = (uint32_t)k;
     }
@@ -608,6 +611,7 @@ struct NarrowOut {
     unsigned long long* vf_count;
     unsigned long long* ee_count;
     unsigned long long* rejections;
+    uint32_t nb;  // bits per vertex id in the contact keys
 };
 
 __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
@@ -645,14 +649,14 @@ __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, 
             atomicMin(&o.dist[ids.z], db);
             if (kind == 0) {
                 if (vertex_feasible(w, xv, fid))
-                    push_contact(0, v, fid, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+                    push_contact(0, v, fid, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
             } else if (kind == 1) {
                 if (edge_feasible(w, xv, fid)) {
                     uint2 ev = w.edges[fid];
-                    push_contact(1, v, ev.x, ev.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+                    push_contact(1, v, ev.x, ev.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
                 }
             } else {
-                push_contact(2, v, ids.x, ids.y, ids.z, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+                push_contact(2, v, ids.x, ids.y, ids.z, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
             }
         } else {
             unsigned long long kk = k - n_vf;
@@ -682,14 +686,14 @@ __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, 
                 continue;
             if (end_a >= 0 && end_b >= 0)
                 push_contact(0, (uint32_t)end_a, (uint32_t)end_b, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap,
-                             o.count);
+                             o.count, o.nb);
             else if (end_a >= 0)
-                push_contact(1, (uint32_t)end_a, js.x, js.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+                push_contact(1, (uint32_t)end_a, js.x, js.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
             else if (end_b >= 0)
-                push_contact(1, (uint32_t)end_b, ids.x, ids.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count);
+                push_contact(1, (uint32_t)end_b, ids.x, ids.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
             else
                 push_contact(3, ids.x, ids.y, js.x, js.y, 1e-3 * w.rest_len2[e] * w.rest_len2[f], o.hi, o.lo, o.eps,
-                             o.idx, o.cap, o.count);
+                             o.idx, o.cap, o.count, o.nb);
         }
     }
     for (int s = 16; s > 0; s >>= 1) {
@@ -750,14 +754,14 @@ __device__ bool contact_active(const WorldView& w, uint32_t kind, uint4 v, doubl
 
 __global__ void k_compact(const unsigned long long* hi, const unsigned long long* lo, const uint32_t* idx_sorted,
                           const double* raw_eps, const uint32_t* flag, const uint32_t* pos, size_t n,
-                          uint32_t* c_kind, uint4* c_verts, double* c_eps) {
+                          uint32_t* c_kind, uint4* c_verts, double* c_eps, uint32_t nb) {
+    const unsigned long long m = (1ull << nb) - 1ull;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!flag[i]) continue;
         uint32_t j = pos[i];
         unsigned long long h = hi[i], l = lo[i];
-        c_kind[j] = (uint32_t)(h >> 62);
-        c_verts[j] = make_uint4((uint32_t)((h >> 31) & 0x7fffffffull), (uint32_t)(h & 0x7fffffffull),
-                                (uint32_t)(l >> 32), (uint32_t)(l & 0xffffffffull));
+        c_kind[j] = (uint32_t)(h >> (2 * nb));
+        c_verts[j] = make_uint4((uint32_t)((h >> nb) & m), (uint32_t)(h & m), (uint32_t)(l >> nb), (uint32_t)(l & m));
         c_eps[j] = raw_eps[idx_sorted[i]];
     }
 }
@@ -780,8 +784,9 @@ __global__ void k_contact_finalize(WorldView w, const uint32_t* c_kind, const ui
 
 // (vertex, contact) keys; sorted, they give every row in ascending contact
 // order, as the reference's incidence lists are (world.rs:386-393).
+// key = vertex << cb | contact index (cb bits hold every contact index)
 __global__ void k_incidence_keys(uint32_t moving, const uint32_t* c_kind, const uint4* c_verts, size_t n,
-                                 unsigned long long* keys, unsigned int* count) {
+                                 unsigned long long* keys, unsigned int* count, uint32_t cb) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint4 v = c_verts[i];
         uint32_t vs[4] = {v.x, v.y, v.z, v.w};
@@ -789,14 +794,15 @@ __global__ void k_incidence_keys(uint32_t moving, const uint32_t* c_kind, const 
         for (uint32_t k = 0; k < cnt; ++k)
             if (vs[k] < moving) {
                 unsigned int slot = atomicAdd(count, 1u);
-                keys[slot] = ((unsigned long long)vs[k] << 32) | (unsigned long long)i;
+                keys[slot] = ((unsigned long long)vs[k] << cb) | (unsigned long long)i;
             }
     }
 }
 
-__global__ void k_incidence_extract(const unsigned long long* keys, size_t n, uint32_t* inc) {
+__global__ void k_incidence_extract(const unsigned long long* keys, size_t n, uint32_t* inc, uint32_t cb) {
+    const unsigned long long m = (1ull << cb) - 1ull;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        inc[i] = (uint32_t)(keys[i] & 0xffffffffull);
+        inc[i] = (uint32_t)(keys[i] & m);
 }
 
 __global__ void k_radii(WorldView w, const unsigned long long* dist, double relaxation, double query_radius,
@@ -1118,6 +1124,10 @@ void World::detect(double query_radius, double radius, double relaxation, double
                                 stream_));
     }
     unsigned long long n_vf = stats_h_.ptr->n_vf, n_ee = stats_h_.ptr->n_ee;
+    // bits per vertex id in the contact keys: the radix sorts below run only
+    // over the 2nb + 2 (hi) and 2nb (lo) bits the keys use
+    uint32_t nb = 1;
+    while ((1ull << nb) < (unsigned long long)n_all_) ++nb;
     // narrow phase
     if (raw_cap_ == 0) raw_cap_ = std::max<size_t>(4096, (size_t)(n_vf + n_ee) / 2 + 4096);
     for (int attempt = 0; attempt < 8; ++attempt) {
@@ -1130,8 +1140,8 @@ void World::detect(double query_radius, double radius, double relaxation, double
         unsigned long long qbits;
         std::memcpy(&qbits, &query_radius, 8);
         k_fill_u64<<<grid_for(n_all_, 256), 256, 0, stream_>>>(dist_bits_.ptr, n_all_, qbits);
-        NarrowOut o{raw_hi_.ptr, raw_lo_.ptr,        raw_eps_.ptr,       raw_idx_.ptr,        raw_cap_,
-                    &sd->n_raw,  dist_bits_.ptr,     &sd->vf_count,      &sd->ee_count,       &sd->rejections};
+        NarrowOut o{raw_hi_.ptr,   raw_lo_.ptr,    raw_eps_.ptr,   raw_idx_.ptr,      raw_cap_, &sd->n_raw,
+                    dist_bits_.ptr, &sd->vf_count, &sd->ee_count, &sd->rejections, nb};
         unsigned long long total = n_vf + n_ee;
         k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee, query_radius,
                                                                     &sd->max_abs_bits, prune ? 1 : 0, o);
@@ -1156,8 +1166,9 @@ void World::detect(double query_radius, double radius, double relaxation, double
         uniq_flag_.reserve(n_raw);
         uniq_pos_.reserve(n_raw);
         size_t need = 0, need2 = 0;
+        const int lo_bits = (int)(2 * nb), hi_bits = (int)(2 * nb + 2);
         cub::DeviceRadixSort::SortPairs(nullptr, need, raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_idx_s_.ptr,
-                                        (int)n_raw, 0, 64, stream_);
+                                        (int)n_raw, 0, hi_bits, stream_);
         cub::DeviceScan::ExclusiveSum(nullptr, need2, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw, stream_);
         need = std::max(need, need2);
         if (need > cub_tmp_bytes_) {
@@ -1165,11 +1176,11 @@ void World::detect(double query_radius, double radius, double relaxation, double
             cub_tmp_bytes_ = need;
         }
         CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.ptr, need, raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr,
-                                                raw_idx_s_.ptr, (int)n_raw, 0, 64, stream_));
+                                                raw_idx_s_.ptr, (int)n_raw, 0, lo_bits, stream_));
         // gather hi in lo order, then stable sort by hi
         k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_idx_s_.ptr, raw_hi_s_.ptr, n_raw);
         CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.ptr, need, raw_hi_s_.ptr, raw_hi_.ptr, raw_idx_s_.ptr,
-                                                raw_idx_.ptr, (int)n_raw, 0, 64, stream_));
+                                                raw_idx_.ptr, (int)n_raw, 0, hi_bits, stream_));
         // raw_hi_ = sorted hi, raw_idx_ = original index; gather lo
         k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_lo_.ptr, raw_idx_.ptr, raw_lo_s_.ptr, n_raw);
         k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, n_raw, uniq_flag_.ptr);
@@ -1185,7 +1196,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
         c_eps_.reserve(n_unique);
         k_compact<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_eps_.ptr,
                                                              uniq_flag_.ptr, uniq_pos_.ptr, n_raw, c_kind_.ptr,
-                                                             c_verts_.ptr, c_eps_.ptr);
+                                                             c_verts_.ptr, c_eps_.ptr, nb);
         launches_ += 4;
     }
     // incidence (moving vertices), active count, radii
@@ -1210,22 +1221,26 @@ void World::detect(double query_radius, double radius, double relaxation, double
     if (n_unique > 0) {
         inc_keys_.reserve(n_inc_bound);
         inc_keys_s_.reserve(n_inc_bound);
+        uint32_t cb = 1;  // bits per contact index in the incidence keys
+        while ((1ull << cb) < (unsigned long long)n_unique) ++cb;
+        const int inc_bits = (int)(nb + cb);
         k_incidence_keys<<<grid_for(n_unique, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
-                                                                        n_unique, inc_keys_.ptr, inc_cursor_.ptr);
+                                                                        n_unique, inc_keys_.ptr, inc_cursor_.ptr, cb);
         ++launches_;
         uint32_t n_inc = 0;
         CC_CUDA(cudaMemcpyAsync(&n_inc, inc_cursor_.ptr, 4, cudaMemcpyDeviceToHost, stream_));
         CC_CUDA(cudaStreamSynchronize(stream_));
         if (n_inc > 0) {
             size_t need = 0;
-            cub::DeviceRadixSort::SortKeys(nullptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0, 64, stream_);
+            cub::DeviceRadixSort::SortKeys(nullptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0, inc_bits,
+                                           stream_);
             if (need > cub_tmp_bytes_) {
                     cub_tmp_.reserve(need);
                 cub_tmp_bytes_ = need;
             }
             CC_CUDA(cub::DeviceRadixSort::SortKeys(cub_tmp_.ptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0,
-                                                   64, stream_));
-            k_incidence_extract<<<grid_for(n_inc, 256), 256, 0, stream_>>>(inc_keys_s_.ptr, n_inc, inc_.ptr);
+                                                   inc_bits, stream_));
+            k_incidence_extract<<<grid_for(n_inc, 256), 256, 0, stream_>>>(inc_keys_s_.ptr, n_inc, inc_.ptr, cb);
             ++launches_;
         }
     }

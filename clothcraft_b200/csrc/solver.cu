@@ -593,9 +593,11 @@ struct cc_solver {
 // Project autotuner: time one full colour sweep per candidate group width on
 // a backup of the positions (restored after each trial) and keep the fastest.
 void cc_solver::autotune(const SweepView& sv_in) {
-    // lanes per vertex | register cap (3 or 4 resident 128-thread blocks per SM) << 8
-    static const int kCandidates[] = {1 | 3 << 8, 2 | 3 << 8, 4 | 3 << 8,  4 | 4 << 8,  4 | 5 << 8, 8 | 3 << 8,
-                                      8 | 4 << 8, 8 | 5 << 8, 16 | 3 << 8, 16 | 4 << 8, 32 | 3 << 8};
+    // lanes per vertex | register cap (resident 128-thread blocks per SM: 3, 4, 5,
+    // 6 or 8; above 3 the compiler spills to local memory) << 8
+    static const int kCandidates[] = {1 | 3 << 8,  2 | 3 << 8,  4 | 3 << 8,  4 | 4 << 8,  4 | 5 << 8,  4 | 6 << 8,
+                                      8 | 3 << 8,  8 | 4 << 8,  8 | 5 << 8,  8 | 6 << 8,  8 | 8 << 8,  16 | 3 << 8,
+                                      16 | 4 << 8, 16 | 6 << 8, 16 | 8 << 8, 32 | 3 << 8};
     SweepView sv = sv_in;  // trial sweeps never skip and count into a scratch counter
     sv.skip_at = nullptr;
     sv.clipped = &sc.ptr->clipped;
@@ -1256,11 +1258,11 @@ int32_t cc_solver_set_profiling(cc_solver* s, int32_t enable) {
 }
 int32_t cc_solver_set_lanes(cc_solver* s, int32_t lanes) {
     int32_t g = lanes & 0xff, cap = lanes >> 8;
-    if (!(g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) || cap < 0 || cap > 5 ||
-        (g == 0 && cap != 0) || (cap != 0 && cap < 3))
+    if (!(g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) ||
+        !(cap == 0 || cap == 3 || cap == 4 || cap == 5 || cap == 6 || cap == 8) || (g == 0 && cap != 0))
         return s->fail(Failure{CC_ERR_INVALID_ARGUMENT,
                                "lanes must be 0 (autotune) or a power of two up to 32, optionally | cap << 8 with "
-                               "cap in 3..5"});
+                               "cap 3, 4, 5, 6 or 8"});
     s->lanes = lanes == 0 ? 0 : (g | (cap ? cap : 3) << 8);
     return CC_OK;
 }

@@ -681,7 +681,9 @@ static void launch_g(const SweepView& s, const uint32_t* order, uint32_t count, 
     constexpr int B = 128;
     uint64_t threads = (uint64_t)count * G;
     unsigned grid = (unsigned)((threads + B - 1) / B);
-    if (minb >= 5) k_sweep<G, B, 5><<<grid, B, 0, st>>>(s, order, count);
+    if (minb >= 8) k_sweep<G, B, 8><<<grid, B, 0, st>>>(s, order, count);
+    else if (minb >= 6) k_sweep<G, B, 6><<<grid, B, 0, st>>>(s, order, count);
+    else if (minb == 5) k_sweep<G, B, 5><<<grid, B, 0, st>>>(s, order, count);
     else if (minb == 4) k_sweep<G, B, 4><<<grid, B, 0, st>>>(s, order, count);
     else k_sweep<G, B, 3><<<grid, B, 0, st>>>(s, order, count);
 }

@@ -267,8 +267,9 @@ void* cc_solver_stream(const cc_solver* solver);
  * cc_metrics.sweep_ms reports their summed device time. */
 int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
 /* Threads that cooperate on one vertex's local solve (1, 2, 4, 8, 16 or 32),
- * optionally | (cap << 8) with cap = 3, 4 or 5 resident 128-thread blocks per
- * SM (a register budget; default 3); 0 (the default) lets the solver time the
+ * optionally | (cap << 8) with cap = 3, 4, 5, 6 or 8 resident 128-thread
+ * blocks per SM (a register budget; default 3; above 3 registers spill to
+ * local memory); 0 (the default) lets the solver time the
  * candidates on its first step and keep the fastest. get_lanes returns the
  * same encoding. Two solvers take bitwise-identical steps only with the same
  * setting. No reference counterpart (the wgpu backend always uses a 32-lane

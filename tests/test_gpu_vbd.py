@@ -213,3 +213,31 @@ def test_resident_stepping_equals_host_stepping():
         b.step_resident(st)
     xb, vb, tb = b.get_state()
     assert np.array_equal(x, xb) and np.array_equal(v, vb) and t == tb
+
+
+@pytest.mark.parametrize("lanes", [4, 8, 16])
+def test_register_caps_give_identical_steps(lanes):
+    """The register cap (resident blocks per SM, with local-memory spills above
+    3) changes only the schedule: every cap gives the bits of cap 3."""
+    sc = contact_scene(12, seed=8)
+    st = sc.settings.to_c()
+    ref = VbdSolver(sc).set_lanes(lanes | 3 << 8)
+    x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
+    ref.set_state(x, v, t)
+    for _ in range(3):
+        ref.step_resident(st)
+    xr, vr, _ = ref.get_state()
+    for cap in (4, 5, 6, 8):
+        s = VbdSolver(sc).set_lanes(lanes | cap << 8)
+        s.set_state(x, v, t)
+        for _ in range(3):
+            s.step_resident(st)
+        xs, vs, _ = s.get_state()
+        assert np.array_equal(xs, xr) and np.array_equal(vs, vr), cap
+
+
+def test_invalid_register_cap_is_rejected():
+    s = VbdSolver(contact_scene(8, seed=1))
+    for bad in (4 | 7 << 8, 4 | 2 << 8, 4 | 9 << 8, 3, 0 | 4 << 8):
+        with pytest.raises(VbdError):
+            s.set_lanes(bad)
