@@ -373,13 +373,17 @@ def main():
         su = step_settings(sc, mode, acceleration=0.0)
         solver_u = make(mode, acceleration=0.0)
         unacc[mode] = leg(solver_u, lambda: solver_u.step_resident(su), K)
-    # ---- end to end through cc_solver_step with host arrays (learned)
+    # ---- end to end through cc_solver_step with host arrays in pinned memory
+    # (learned): the caller's x and v go in and come back every step
     e2e_solver = make(1)
     x, v, t = e2e_solver.get_state()
-    state = {"x": x, "v": v, "t": t}
+    xh = torch.empty((sc.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    vh = torch.empty((sc.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    xh[:], vh[:] = x, v
+    state = {"t": t}
 
     def host_step():
-        state["x"], state["v"], state["t"], m = e2e_solver.step(state["x"], state["v"], state["t"], st_l)
+        state["t"], m = e2e_solver.step_into(xh, vh, state["t"], st_l)
         return m
 
     t_e2e, mets_e2e = leg(e2e_solver, host_step, K)
@@ -486,8 +490,9 @@ def main():
             "sweep_share_of_step": sweep_ms / max(sum(m["gpu_compute_ms"] for m in mets_prof), 1e-9),
         },
         "cpu_baseline": cpu,
-        "e2e": {"value": world * K / (t_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 2 * sc.n * 32,
-                "d2h_bytes_per_step": 2 * sc.n * 32, "mean_iterations": float(np.mean(iters(mets_e2e)))},
+        "e2e": {"value": world * K / (t_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 2 * sc.n * 24,
+                "d2h_bytes_per_step": 2 * sc.n * 24, "mean_iterations": float(np.mean(iters(mets_e2e))),
+                "host_memory": "pinned, [n][3] float64 x and v, stepped in place (VbdSolver.step_into)"},
         "gpu_launches": int(sum(m["kernel_launches"] for m in mets_l)),
         "lanes_per_vertex": int(L.cc_solver_get_lanes(learned.h)) & 0xff,
         "blocks_per_sm_cap": int(L.cc_solver_get_lanes(learned.h)) >> 8,

@@ -167,6 +167,42 @@ __global__ void k_accelerate(uint32_t n, const uint8_t* pinned, ContactsView c, 
     }
 }
 
+// The caller's x and v ([n][3] doubles) are copied as they are, straight from
+// or into the caller's memory (DMA when it is pinned), and converted to and
+// from the padded device layout on the GPU.
+__global__ void k_unpack_state(uint32_t n, const double* io, double4* x, double4* v) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double* a = io + 3 * (size_t)i;
+        const double* b = io + 3 * ((size_t)n + i);
+        x[i] = make_double4(a[0], a[1], a[2], 0.0);
+        v[i] = make_double4(b[0], b[1], b[2], 0.0);
+    }
+}
+
+__global__ void k_pack_state(uint32_t n, const double4* x, const double4* v, double* io) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double4 a = x[i], b = v[i];
+        double* p = io + 3 * (size_t)i;
+        double* q = io + 3 * ((size_t)n + i);
+        p[0] = a.x;
+        p[1] = a.y;
+        p[2] = a.z;
+        q[0] = b.x;
+        q[1] = b.y;
+        q[2] = b.z;
+    }
+}
+
+void launch_unpack_state(size_t n, const double* io, double4* x, double4* v, cudaStream_t st) {
+    k_unpack_state<<<grid_for(n, 256), 256, 0, st>>>((uint32_t)n, io, x, v);
+    CC_CUDA(cudaGetLastError());
+}
+
+void launch_pack_state(size_t n, const double4* x, const double4* v, double* io, cudaStream_t st) {
+    k_pack_state<<<grid_for(n, 256), 256, 0, st>>>((uint32_t)n, x, v, io);
+    CC_CUDA(cudaGetLastError());
+}
+
 // Conservative warm start (src/vbd.rs:316-324)
 __global__ void k_warm_start(uint32_t n, const uint8_t* pinned, const double4* guess, ContactsView c, double4* x,
                              unsigned int* clipped) {
@@ -405,6 +441,7 @@ struct cc_solver {
     DBuf<StepScalars> sc;
     Pinned<StepScalars> sc_h;
     Pinned<double4> stage;
+    DBuf<double> io;  // [2][n][3] device copy of a caller's x and v (host layout)
     double time = 0.0;
     bool has_pred = false;
     double pred_time = 0.0, pred_damping = 0.0;
@@ -1223,6 +1260,7 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         h->sc.reserve(1);
         h->sc_h.reserve(1);
         h->stage.reserve(2 * n);
+        h->io.reserve(6 * n);
         h->ext_key.reserve(T);
         h->ext_key_s.reserve(T);
         h->ext_w.reserve(T);
@@ -1271,28 +1309,19 @@ cc_world* cc_solver_world(cc_solver* s) { return &s->world_view; }
 
 static void upload_state(cc_solver* s, const double* x, const double* v) {
     size_t n = s->n;
-    for (size_t i = 0; i < n; ++i) {
-        s->stage.ptr[i] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], 0.0);
-        s->stage.ptr[n + i] = make_double4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0);
-    }
-    CC_CUDA(cudaMemcpyAsync(s->x0.ptr, s->stage.ptr, n * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
-    CC_CUDA(cudaMemcpyAsync(s->v0.ptr, s->stage.ptr + n, n * sizeof(double4), cudaMemcpyHostToDevice, s->stream));
+    if (n == 0) return;
+    CC_CUDA(cudaMemcpyAsync(s->io.ptr, x, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CC_CUDA(cudaMemcpyAsync(s->io.ptr + 3 * n, v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    launch_unpack_state(n, s->io.ptr, s->x0.ptr, s->v0.ptr, s->stream);
 }
 
 static void download_state(cc_solver* s, double* x, double* v) {
     size_t n = s->n;
-    CC_CUDA(cudaMemcpyAsync(s->stage.ptr, s->x0.ptr, n * sizeof(double4), cudaMemcpyDeviceToHost, s->stream));
-    CC_CUDA(cudaMemcpyAsync(s->stage.ptr + n, s->v0.ptr, n * sizeof(double4), cudaMemcpyDeviceToHost, s->stream));
+    if (n == 0) return;
+    launch_pack_state(n, s->x0.ptr, s->v0.ptr, s->io.ptr, s->stream);
+    CC_CUDA(cudaMemcpyAsync(x, s->io.ptr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CC_CUDA(cudaMemcpyAsync(v, s->io.ptr + 3 * n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CC_CUDA(cudaStreamSynchronize(s->stream));
-    for (size_t i = 0; i < n; ++i) {
-        double4 a = s->stage.ptr[i], b = s->stage.ptr[n + i];
-        x[3 * i] = a.x;
-        x[3 * i + 1] = a.y;
-        x[3 * i + 2] = a.z;
-        v[3 * i] = b.x;
-        v[3 * i + 1] = b.y;
-        v[3 * i + 2] = b.z;
-    }
 }
 
 int32_t cc_solver_set_state(cc_solver* s, const double* x, const double* v, double time) {

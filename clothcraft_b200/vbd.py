@@ -233,6 +233,24 @@ class VbdSolver:
             raise self._err(rc)
         return x, v, t.value, m.as_dict()
 
+    def step_into(self, x, v, time, settings, grab=None):
+        """One step from host arrays, in place: x and v (C-contiguous float64
+        [n, 3]; pinned memory makes the copies plain DMA) receive the new
+        state, only when the step succeeds. Returns (time, metrics)."""
+        for a in (x, v):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                    and a.flags.writeable and a.shape == (self.n, 3)):
+                raise ValueError("step_into needs writable C-contiguous float64 arrays of shape (%d, 3)" % self.n)
+        t = C.c_double(time)
+        m = cc_metrics()
+        s = _settings_c(settings)
+        g = _grab_c(grab)
+        rc = native.load().cc_solver_step(self.h, _f64p(x), _f64p(v), C.byref(t), C.byref(s), _ref(g, cc_grab),
+                                          C.byref(m))
+        if rc != 0:
+            raise self._err(rc)
+        return t.value, m.as_dict()
+
     # device-resident stepping
     def set_state(self, x, v, time):
         x = abi.as_f64(x)

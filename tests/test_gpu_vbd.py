@@ -241,3 +241,29 @@ def test_invalid_register_cap_is_rejected():
     for bad in (4 | 7 << 8, 4 | 2 << 8, 4 | 9 << 8, 3, 0 | 4 << 8):
         with pytest.raises(VbdError):
             s.set_lanes(bad)
+
+
+def test_step_into_pinned_arrays_equals_step():
+    """In-place stepping on pinned host arrays (the caller's memory is copied
+    as it is and converted on the GPU) gives the bits of `step`, and a failed
+    step leaves the caller's arrays untouched."""
+    import torch
+
+    sc = contact_scene(12, seed=8)
+    st = sc.settings.to_c()
+    a = VbdSolver(sc).set_lanes(4)
+    b = VbdSolver(sc).set_lanes(4)
+    xh = torch.empty((sc.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    vh = torch.empty((sc.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    xh[:], vh[:] = sc.x0, sc.v0
+    x, v, ta, tb = sc.x0.copy(), sc.v0.copy(), 0.0, 0.0
+    for _ in range(4):
+        x, v, ta, _ = a.step(x, v, ta, st)
+        tb, _ = b.step_into(xh, vh, tb, st)
+    assert np.array_equal(x, xh) and np.array_equal(v, vh) and ta == tb
+    before = (xh.copy(), vh.copy())
+    with pytest.raises(VbdError):
+        b.step_into(xh, vh, tb, scenes.StepSettings(dt=0.1).to_c())
+    assert np.array_equal(xh, before[0]) and np.array_equal(vh, before[1])
+    with pytest.raises(ValueError):
+        b.step_into(xh[:, :2], vh, tb, st)
