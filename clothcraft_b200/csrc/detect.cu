@@ -1035,52 +1035,6 @@ static void raise_device_error(unsigned int e) {
     if (e & DERR_STACK_OVERFLOW) throw Failure{CC_ERR_CUDA, "OGC LBVH traversal stack overflow"};
 }
 
-static uint32_t bits_for(size_t n) {  // smallest b >= 1 with 2^b >= n
-    uint32_t b = 1;
-    while ((1ull << b) < (unsigned long long)n) ++b;
-    return b;
-}
-
-__global__ void k_pair_keys(const uint2* pairs, size_t n, uint32_t sb, unsigned long long* keys) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        uint2 p = pairs[i];
-        keys[i] = ((unsigned long long)p.x << sb) | (unsigned long long)p.y;
-    }
-}
-
-__global__ void k_pair_unkeys(const unsigned long long* keys, size_t n, uint32_t sb, uint2* pairs) {
-    const unsigned long long m = (1ull << sb) - 1ull;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        unsigned long long k = keys[i];
-        pairs[i] = make_uint2((uint32_t)(k >> sb), (uint32_t)(k & m));
-    }
-}
-
-// Order candidate pairs by (first, second). The queries append pairs in
-// atomic order, so a warp of the narrow phase would gather 32 unrelated
-// pairs; sorted, neighbouring threads share the query primitive and nearby
-// partners. Runs once per rebuild; every narrow phase until the next rebuild
-// reads the sorted list. The order does not change any result: contacts are
-// sorted canonically afterwards and the distance minima do not depend on it.
-void World::sort_pairs(uint2* pairs, size_t n, uint32_t first_bits, uint32_t second_bits) {
-    if (n < 2) return;
-    pair_keys_.reserve(n);
-    pair_keys_s_.reserve(n);
-    k_pair_keys<<<grid_for(n, 256), 256, 0, stream_>>>(pairs, n, second_bits, pair_keys_.ptr);
-    const int bits = (int)(first_bits + second_bits);
-    size_t need = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, need, pair_keys_.ptr, pair_keys_s_.ptr, (int)n, 0, bits, stream_);
-    if (need > cub_tmp_bytes_) {
-        cub_tmp_.reserve(need);
-        cub_tmp_bytes_ = need;
-    }
-    CC_CUDA(cub::DeviceRadixSort::SortKeys(cub_tmp_.ptr, need, pair_keys_.ptr, pair_keys_s_.ptr, (int)n, 0, bits,
-                                           stream_));
-    k_pair_unkeys<<<grid_for(n, 256), 256, 0, stream_>>>(pair_keys_s_.ptr, n, second_bits, pairs);
-    launches_ += 2;
-    CC_CUDA(cudaGetLastError());
-}
-
 void World::build_candidates(double R, double skin) {
     double search = R + 2.0 * skin + 1e-12;  // candidates.rs:23-28
     double search2 = search * search;
@@ -1119,11 +1073,7 @@ void World::build_candidates(double R, double skin) {
             ee_.release();
             grow = true;
         }
-        if (!grow) {
-            sort_pairs(vf_.ptr, stats_h_.ptr->n_vf, bits_for(n_all_), bits_for(n_tri_));
-            sort_pairs(ee_.ptr, stats_h_.ptr->n_ee, bits_for(n_edge_), bits_for(n_edge_));
-            return;
-        }
+        if (!grow) return;
     }
     throw Failure{CC_ERR_CUDA, "OGC candidate buffers could not be sized"};
 }
@@ -1176,7 +1126,8 @@ void World::detect(double query_radius, double radius, double relaxation, double
     unsigned long long n_vf = stats_h_.ptr->n_vf, n_ee = stats_h_.ptr->n_ee;
     // bits per vertex id in the contact keys: the radix sorts below run only
     // over the 2nb + 2 (hi) and 2nb (lo) bits the keys use
-    const uint32_t nb = bits_for(n_all_);
+    uint32_t nb = 1;
+    while ((1ull << nb) < (unsigned long long)n_all_) ++nb;
     // narrow phase
     if (raw_cap_ == 0) raw_cap_ = std::max<size_t>(4096, (size_t)(n_vf + n_ee) / 2 + 4096);
     for (int attempt = 0; attempt < 8; ++attempt) {
@@ -1270,7 +1221,8 @@ void World::detect(double query_radius, double radius, double relaxation, double
     if (n_unique > 0) {
         inc_keys_.reserve(n_inc_bound);
         inc_keys_s_.reserve(n_inc_bound);
-        const uint32_t cb = bits_for(n_unique);  // bits per contact index in the incidence keys
+        uint32_t cb = 1;  // bits per contact index in the incidence keys
+        while ((1ull << cb) < (unsigned long long)n_unique) ++cb;
         const int inc_bits = (int)(nb + cb);
         k_incidence_keys<<<grid_for(n_unique, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
                                                                         n_unique, inc_keys_.ptr, inc_cursor_.ptr, cb);

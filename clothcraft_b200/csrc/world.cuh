@@ -129,7 +129,6 @@ class World {
     WorldView view() const;
     void refit(bool check_fixed);
     void build_candidates(double R, double skin);
-    void sort_pairs(uint2* pairs, size_t n, uint32_t first_bits, uint32_t second_bits);
     void sync_stats();
 
     cudaStream_t stream_;
@@ -153,7 +152,6 @@ class World {
     DBuf<double4> cache_centers_;
     DBuf<uint2> vf_, ee_;
     size_t vf_cap_ = 0, ee_cap_ = 0;
-    DBuf<unsigned long long> pair_keys_, pair_keys_s_;  // candidate sort (after a rebuild)
 
     // narrow phase + canonical set
     DBuf<unsigned long long> raw_hi_, raw_lo_, raw_hi_s_, raw_lo_s_;
