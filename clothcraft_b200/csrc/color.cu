@@ -64,7 +64,15 @@ __device__ __forceinline__ uint32_t greedy_color(const ColorView& g, const uint1
 // iterated Jacobi-style (read all, barrier, write changes) until no colour
 // changes. A chunk converges in at most (its internal descending chain + 1)
 // rounds <= kChunk + 1, so the loop is bounded; starting from the previous
-// colouring a chunk usually settles in one or two rounds.
+// colouring a chunk usually settles in a few rounds.
+//
+// Per chunk each thread first folds the colours of its vertex's final lower
+// neighbours (index below the chunk) into a 64-bit mask, and keeps the
+// in-chunk lower neighbours (at most kInner, as chunk-local indices) in
+// shared memory; the rounds then read only shared memory: the mask, those
+// indices and the chunk's current colours. A vertex with more in-chunk lower
+// neighbours, or with a colour >= 64 around it, takes the full rule
+// (greedy_color) every round instead. Both give the rule's exact value.
 //
 // The walk starts at the chunk of `first[0]`, the lowest vertex whose rule
 // does not hold for the previous colouring (k_color_probe): every vertex
@@ -72,10 +80,13 @@ __device__ __forceinline__ uint32_t greedy_color(const ColorView& g, const uint1
 // is final too. When the whole colouring fits (n <= kSmemColors) it is kept
 // in shared memory for the walk.
 constexpr int kChunk = 1024;
-constexpr uint32_t kSmemColors = 96 * 1024;  // 192 KB of uint16 colours
+constexpr int kInner = 16;
+constexpr uint32_t kSmemColors = 90 * 1024;  // 180 KB of uint16 colours (+ 34 KB static)
 __global__ void __launch_bounds__(kChunk) k_color_chunked(ColorView g, uint16_t* col_g, const unsigned int* first,
                                                          unsigned int* rounds_out, unsigned int* err) {
     extern __shared__ uint16_t col_s[];
+    __shared__ uint16_t inner[kInner][kChunk];  // chunk-local indices of in-chunk lower neighbours
+    __shared__ uint16_t chunk_col[kChunk];      // the chunk's current colours
     uint32_t start = *first;
     if (start >= g.n) {  // already a fixed point
         if (threadIdx.x == 0) *rounds_out = 0;
@@ -88,25 +99,68 @@ __global__ void __launch_bounds__(kChunk) k_color_chunked(ColorView g, uint16_t*
         __syncthreads();
         col = col_s;
     }
+    const uint32_t t = threadIdx.x;
     unsigned int rounds = 0;
     for (uint32_t base = (start / kChunk) * kChunk; base < g.n; base += kChunk) {
-        uint32_t v = base + threadIdx.x;
+        const uint32_t v = base + t;
+        const bool live = v < g.n;
+        // set-up: final colours below the chunk into a mask, in-chunk lower
+        // neighbours into shared memory
+        unsigned long long outer = 0;
+        bool slow = false;
+        uint32_t ninner = 0;
+        auto visit = [&](uint32_t u) {
+            if (u >= v) return;
+            if (u < base) {
+                mark(outer, col[u], slow);
+            } else if (ninner < kInner) {
+                inner[ninner++][t] = (uint16_t)(u - base);
+            } else {
+                slow = true;
+            }
+        };
+        if (live) {
+            for (uint32_t k = g.lo_off[v]; k < g.lo_off[v + 1]; ++k) visit(g.lo[k]);
+            for (uint32_t k = g.contacts.inc_off[v]; k < g.contacts.inc_off[v + 1]; ++k) {
+                uint32_t c = g.contacts.inc[k];
+                uint32_t kind = g.contacts.kind[c];
+                uint4 cv = g.contacts.verts[c];
+                uint32_t ids[4] = {cv.x, cv.y, cv.z, cv.w};
+                uint32_t cnt = kind == 0 ? 2u : (kind == 1 ? 3u : 4u);
+                for (uint32_t j = 0; j < cnt; ++j) visit(ids[j]);
+            }
+            if (g.grab_active && (g.grab_v[0] == v || g.grab_v[1] == v || g.grab_v[2] == v))
+                for (int j = 0; j < 3; ++j) visit(g.grab_v[j]);
+            chunk_col[t] = col[v];
+        }
+        __syncthreads();
         int r = 0;
         for (; r <= kChunk + 1; ++r) {
-            uint32_t c = v < g.n ? greedy_color(g, col, v) : 0u;
+            uint32_t c = 0u;
+            if (live) {
+                unsigned long long mask = outer;
+                bool high = slow;
+                for (uint32_t j = 0; j < ninner; ++j) mark(mask, chunk_col[inner[j][t]], high);
+                // colours >= 64 around v, or all of 0..63 taken: the full rule
+                if (high || ~mask == 0ull) c = greedy_color(g, col, v);
+                else c = (uint32_t)__ffsll((long long)~mask) - 1;
+            }
             __syncthreads();
-            int changed = (v < g.n && c != col[v]) ? 1 : 0;
-            if (changed) col[v] = (uint16_t)c;
+            int changed = (live && c != chunk_col[t]) ? 1 : 0;
+            if (changed) {
+                chunk_col[t] = (uint16_t)c;
+                col[v] = (uint16_t)c;
+            }
             ++rounds;
             if (!__syncthreads_or(changed)) break;
         }
-        if (r > kChunk + 1 && threadIdx.x == 0) atomicOr(err, 1u);
+        if (r > kChunk + 1 && t == 0) atomicOr(err, 1u);
     }
     if (smem) {
         __syncthreads();
         for (uint32_t i = (start / kChunk) * kChunk + threadIdx.x; i < g.n; i += kChunk) col_g[i] = col_s[i];
     }
-    if (threadIdx.x == 0) *rounds_out = rounds;
+    if (t == 0) *rounds_out = rounds;
 }
 
 // Lowest vertex whose greedy rule fails for the current colouring.

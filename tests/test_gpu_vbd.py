@@ -91,6 +91,30 @@ def test_coloring_matches_sequential_greedy():
         assert np.array_equal(cg, co)
 
 
+def test_coloring_matches_sequential_greedy_above_the_shared_memory_size():
+    """102,400 vertices (more than the 92,160 colours the walk keeps in shared
+    memory, so colours stay in global memory) folded into two layers 1 mm
+    apart: ~10^5 contact co-vertex edges between the layers."""
+    sc = scenes.small_sheet(320, seed=1, obstacle=False, side=1.0, radius=0.0005, pins=())
+    x = sc.x0.copy()
+    right = x[:, 0] > 0.0
+    x[right, 0] = -x[right, 0]
+    x[right, 1] += 0.001
+    g = VbdSolver(sc)
+    o = oracle.Solver(sc, threads=8)
+    x_all = g.positions(x)
+    cg, ng = g.colors(x_all, 0.002, sc.settings)
+    co, no = o.colors(x_all, 0.002, sc.settings.ogc_c())
+    assert ng == no and ng > 4
+    assert np.array_equal(cg, co)
+    # again from the previous colouring, after a small displacement
+    x[::7, 1] += 2e-4
+    x_all = g.positions(x)
+    cg, ng = g.colors(x_all, 0.002, sc.settings)
+    co, no = o.colors(x_all, 0.002, sc.settings.ogc_c())
+    assert ng == no and np.array_equal(cg, co)
+
+
 @pytest.mark.parametrize("maker", [lambda: scenes.small_sheet(16, seed=2),
                                    lambda: contact_scene(16, seed=4)])
 def test_one_step_positions_within_1e5_m(maker):
