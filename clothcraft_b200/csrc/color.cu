@@ -10,7 +10,7 @@
 // longest descending chain, and contact edges between folded layers make
 // chains of length ~n; k_color_chunked below bounds the work by walking
 // index-ordered chunks instead.
-#include <cub/device/device_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
 
 #include "color.cuh"
 
@@ -177,12 +177,8 @@ __global__ void k_color_count(uint32_t n, const uint16_t* col, uint32_t* counts)
         atomicAdd(&counts[col[v]], 1u);
 }
 
-__global__ void k_color_scatter(uint32_t n, const uint16_t* col, const uint32_t* offsets, uint32_t* cursor,
-                                uint32_t* order) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        uint32_t c = col[v];
-        order[offsets[c] + atomicAdd(&cursor[c], 1u)] = v;
-    }
+__global__ void k_iota(uint32_t n, uint32_t* out) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) out[v] = v;
 }
 
 void Coloring::init(uint32_t n, cudaStream_t s) {
@@ -190,13 +186,14 @@ void Coloring::init(uint32_t n, cudaStream_t s) {
     a_.reserve(n);
     b_.reserve(n);
     order_.reserve(n);
+    iota_.reserve(n);
     counts_.reserve(kMaxColors);
-    offsets_.reserve(kMaxColors);
-    cursor_.reserve(kMaxColors);
     changed_.reserve(kBatch);
     changed_h_.reserve(kBatch);
     counts_h_.reserve(kMaxColors);
     CC_CUDA(cudaMemsetAsync(a_.ptr, 0, n * sizeof(uint16_t), s));
+    if (n) k_iota<<<grid_for(n, 256), 256, 0, s>>>(n, iota_.ptr);
+    CC_CUDA(cudaGetLastError());
     cur_ = a_.ptr;
 }
 
@@ -221,7 +218,6 @@ void Coloring::compute(const ColorView& view, cudaStream_t s) {
     launches_ += 2;
     CC_CUDA(cudaGetLastError());
     CC_CUDA(cudaMemsetAsync(counts_.ptr, 0, kMaxColors * sizeof(uint32_t), s));
-    CC_CUDA(cudaMemsetAsync(cursor_.ptr, 0, kMaxColors * sizeof(uint32_t), s));
     k_color_count<<<grid_for(n, 256), 256, 0, s>>>(n, cur_, counts_.ptr);
     CC_CUDA(cudaMemcpyAsync(counts_h_.ptr, counts_.ptr, kMaxColors * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     CC_CUDA(cudaMemcpyAsync(changed_h_.ptr, changed_.ptr, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
@@ -234,9 +230,20 @@ void Coloring::compute(const ColorView& view, cudaStream_t s) {
     if (n_colors_ >= kMaxColors) throw Failure{CC_ERR_CUDA, "colour limit exceeded"};
     offsets_h_.assign(n_colors_ + 1, 0);
     for (uint32_t c = 0; c < n_colors_; ++c) offsets_h_[c + 1] = offsets_h_[c] + counts_h_.ptr[c];
-    CC_CUDA(cudaMemcpyAsync(offsets_.ptr, offsets_h_.data(), (n_colors_ + 1) * sizeof(uint32_t),
-                            cudaMemcpyHostToDevice, s));
-    k_color_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, cur_, offsets_.ptr, cursor_.ptr, order_.ptr);
+    // vertices grouped by colour, in index order within a colour (a stable
+    // sort on the colour bits): a warp's vertices are neighbours in the mesh
+    // order, so the sweep's gathers share cache lines. The order within a
+    // colour does not change any result (no two vertices of a colour interact).
+    int bits = 1;
+    while ((1u << bits) < n_colors_) ++bits;
+    size_t need = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, need, cur_, b_.ptr, iota_.ptr, order_.ptr, (int)n, 0, bits, s);
+    if (need > sort_tmp_bytes_) {
+        sort_tmp_.reserve(need);
+        sort_tmp_bytes_ = need;
+    }
+    CC_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_.ptr, need, cur_, b_.ptr, iota_.ptr, order_.ptr, (int)n, 0, bits,
+                                            s));
     launches_ += 2;
     CC_CUDA(cudaGetLastError());
 }

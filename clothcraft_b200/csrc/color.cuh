@@ -33,7 +33,9 @@ class Coloring {
     uint32_t n_ = 0;
     DBuf<uint16_t> a_, b_;
     uint16_t* cur_ = nullptr;
-    DBuf<uint32_t> order_, counts_, offsets_, cursor_;
+    DBuf<uint32_t> order_, counts_, iota_;
+    DBuf<unsigned char> sort_tmp_;
+    size_t sort_tmp_bytes_ = 0;
     DBuf<unsigned int> changed_;
     Pinned<unsigned int> changed_h_;
     Pinned<uint32_t> counts_h_;
