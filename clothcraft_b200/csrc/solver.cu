@@ -141,6 +141,12 @@ __global__ void k_copy_positions(uint32_t n, const double4* src, double4* dst) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = src[i];
 }
 
+// Lanes per vertex of the residual evaluation (k_grad_sq, one launch over all
+// vertices): 4 is the fastest measured on the fold (36 us per launch against 50
+// with 8), whatever the sweep's variant; the residual's value does not depend on it
+// beyond the last bits of its sums.
+constexpr int kResidualLanes = 4;
+
 // Chebyshev step after iteration `it` (no reference counterpart):
 // x = w (x_sweep - x_prev2) + x_prev2 on free vertices, clipped to the OGC
 // ball, from the second iteration of a sequence on (acc_k >= 2); `hist`
@@ -604,7 +610,7 @@ struct cc_solver {
                        const float* features);
     // |grad E|^2 over moving vertices at view.x into `dst` (device).
     void grad_sq_into(const SweepView& view, double* dst, bool project) {
-        launch_grad_sq(view, gsq.ptr, nullptr, 0, lanes ? lanes : (8 | 3 << 8), project, stream);
+        launch_grad_sq(view, gsq.ptr, nullptr, 0, kResidualLanes, project, stream);
         launch_sum_partial(gsq.ptr, n, partial.ptr, nullptr, 0, stream);
         k_store_sum<<<1, 256, 0, stream>>>(partial.ptr, dst);
         own_launches += 3;
@@ -863,7 +869,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                 }
                 ++own_launches;
                 if (checks && ((it + 1) % check_every == 0 || it + 1 == s.iterations)) {
-                    launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, lanes, true, stream);
+                    launch_grad_sq(sv, gsq.ptr, &sc.ptr->stop_at, it, kResidualLanes, true, stream);
                     launch_sum_partial(gsq.ptr, n, partial.ptr, &sc.ptr->stop_at, it, stream);
                     k_residual_rule<<<1, 256, 0, stream>>>(sc.ptr, partial.ptr, it, s.iterations, tol2,
                                                            target_on ? 1 : 0, s.stall_refresh, accelerate ? 1 : 0);
