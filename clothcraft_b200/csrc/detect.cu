@@ -782,27 +782,35 @@ __global__ void k_contact_finalize(WorldView w, const uint32_t* c_kind, const ui
     if ((threadIdx.x & 31) == 0 && a) atomicAdd(active, a);
 }
 
-// (vertex, contact) keys; sorted, they give every row in ascending contact
-// order, as the reference's incidence lists are (world.rs:386-393).
-// key = vertex << cb | contact index (cb bits hold every contact index)
-__global__ void k_incidence_keys(uint32_t moving, const uint32_t* c_kind, const uint4* c_verts, size_t n,
-                                 unsigned long long* keys, unsigned int* count, uint32_t cb) {
+// Incidence rows: every moving vertex's contacts in ascending contact order,
+// as the reference's incidence lists are (world.rs:386-393). Contacts are dealt
+// into their rows (offsets: the exclusive scan of the per-vertex counts) with
+// one atomic cursor per row, then every row is sorted on its own; rows are
+// short (one vertex's contacts), so an insertion sort per thread suffices.
+__global__ void k_incidence_scatter(uint32_t moving, const uint32_t* c_kind, const uint4* c_verts, size_t n,
+                                    const uint32_t* off, uint32_t* cursor, uint32_t* inc) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint4 v = c_verts[i];
         uint32_t vs[4] = {v.x, v.y, v.z, v.w};
         uint32_t cnt = kind_count(c_kind[i]);
         for (uint32_t k = 0; k < cnt; ++k)
-            if (vs[k] < moving) {
-                unsigned int slot = atomicAdd(count, 1u);
-                keys[slot] = ((unsigned long long)vs[k] << cb) | (unsigned long long)i;
-            }
+            if (vs[k] < moving) inc[off[vs[k]] + atomicAdd(&cursor[vs[k]], 1u)] = (uint32_t)i;
     }
 }
 
-__global__ void k_incidence_extract(const unsigned long long* keys, size_t n, uint32_t* inc, uint32_t cb) {
-    const unsigned long long m = (1ull << cb) - 1ull;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        inc[i] = (uint32_t)(keys[i] & m);
+__global__ void k_incidence_sort_rows(uint32_t moving, const uint32_t* off, uint32_t* inc) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < moving; v += gridDim.x * blockDim.x) {
+        const uint32_t a = off[v], b = off[v + 1];
+        for (uint32_t i = a + 1; i < b; ++i) {
+            uint32_t x = inc[i];
+            uint32_t j = i;
+            while (j > a && inc[j - 1] > x) {
+                inc[j] = inc[j - 1];
+                --j;
+            }
+            inc[j] = x;
+        }
+    }
 }
 
 __global__ void k_radii(WorldView w, const unsigned long long* dist, double relaxation, double query_radius,
@@ -1216,33 +1224,14 @@ void World::detect(double query_radius, double radius, double relaxation, double
         CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1),
                                               stream_));
     }
-    size_t n_inc_bound = 4 * n_unique;
+    size_t n_inc_bound = 4 * n_unique;  // at most 4 moving vertices per contact
     inc_.reserve(std::max<size_t>(n_inc_bound, 1));
     if (n_unique > 0) {
-        inc_keys_.reserve(n_inc_bound);
-        inc_keys_s_.reserve(n_inc_bound);
-        uint32_t cb = 1;  // bits per contact index in the incidence keys
-        while ((1ull << cb) < (unsigned long long)n_unique) ++cb;
-        const int inc_bits = (int)(nb + cb);
-        k_incidence_keys<<<grid_for(n_unique, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
-                                                                        n_unique, inc_keys_.ptr, inc_cursor_.ptr, cb);
-        ++launches_;
-        uint32_t n_inc = 0;
-        CC_CUDA(cudaMemcpyAsync(&n_inc, inc_cursor_.ptr, 4, cudaMemcpyDeviceToHost, stream_));
-        CC_CUDA(cudaStreamSynchronize(stream_));
-        if (n_inc > 0) {
-            size_t need = 0;
-            cub::DeviceRadixSort::SortKeys(nullptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0, inc_bits,
-                                           stream_);
-            if (need > cub_tmp_bytes_) {
-                    cub_tmp_.reserve(need);
-                cub_tmp_bytes_ = need;
-            }
-            CC_CUDA(cub::DeviceRadixSort::SortKeys(cub_tmp_.ptr, need, inc_keys_.ptr, inc_keys_s_.ptr, (int)n_inc, 0,
-                                                   inc_bits, stream_));
-            k_incidence_extract<<<grid_for(n_inc, 256), 256, 0, stream_>>>(inc_keys_s_.ptr, n_inc, inc_.ptr, cb);
-            ++launches_;
-        }
+        k_incidence_scatter<<<grid_for(n_unique, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
+                                                                           n_unique, inc_off_.ptr, inc_cursor_.ptr,
+                                                                           inc_.ptr);
+        k_incidence_sort_rows<<<grid_for(moving_, 256), 256, 0, stream_>>>((uint32_t)moving_, inc_off_.ptr, inc_.ptr);
+        launches_ += 2;
     }
     if (moving_ > 0)
         k_radii<<<grid_for(moving_, 256), 256, 0, stream_>>>(view(), dist_bits_.ptr, relaxation, query_radius,

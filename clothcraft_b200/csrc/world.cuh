@@ -165,7 +165,6 @@ class World {
     DBuf<double> radii_;
     DBuf<double4> centers_;
     DBuf<uint32_t> inc_count_, inc_off_, inc_, inc_cursor_;
-    DBuf<unsigned long long> inc_keys_, inc_keys_s_;
     DBuf<unsigned char> cub_tmp_;
     size_t cub_tmp_bytes_ = 0;
     DBuf<DetectStats> stats_d_;
