@@ -766,8 +766,16 @@ __global__ void k_compact(const unsigned long long* hi, const unsigned long long
     }
 }
 
-__global__ void k_contact_finalize(WorldView w, const uint32_t* c_kind, const uint4* c_verts, size_t n, double r,
-                                   uint32_t* inc_count, unsigned long long* active) {
+// The unique-contact count from the dedup scan: last position + last flag.
+__global__ void k_unique_count(const uint32_t* flag, const uint32_t* pos, size_t n_raw, unsigned long long* out) {
+    *out = (unsigned long long)pos[n_raw - 1] + flag[n_raw - 1];
+}
+
+// n_ptr: the unique-contact count on the device (grids are sized for the raw count)
+__global__ void k_contact_finalize(WorldView w, const uint32_t* c_kind, const uint4* c_verts,
+                                   const unsigned long long* n_ptr, double r, uint32_t* inc_count,
+                                   unsigned long long* active) {
+    const size_t n = (size_t)*n_ptr;
     unsigned long long a = 0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint32_t kind = c_kind[i];
@@ -787,8 +795,10 @@ __global__ void k_contact_finalize(WorldView w, const uint32_t* c_kind, const ui
 // into their rows (offsets: the exclusive scan of the per-vertex counts) with
 // one atomic cursor per row, then every row is sorted on its own; rows are
 // short (one vertex's contacts), so an insertion sort per thread suffices.
-__global__ void k_incidence_scatter(uint32_t moving, const uint32_t* c_kind, const uint4* c_verts, size_t n,
-                                    const uint32_t* off, uint32_t* cursor, uint32_t* inc) {
+__global__ void k_incidence_scatter(uint32_t moving, const uint32_t* c_kind, const uint4* c_verts,
+                                    const unsigned long long* n_ptr, const uint32_t* off, uint32_t* cursor,
+                                    uint32_t* inc) {
+    const size_t n = (size_t)*n_ptr;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint4 v = c_verts[i];
         uint32_t vs[4] = {v.x, v.y, v.z, v.w};
@@ -1165,8 +1175,10 @@ void World::detect(double query_radius, double radius, double relaxation, double
     }
     size_t n_raw = stats_h_.ptr->n_raw;
     if (n_raw > raw_cap_) throw Failure{CC_ERR_CUDA, "OGC contact buffer could not be sized"};
-    // canonical order: stable LSD radix sort on (lo) then (hi)
-    size_t n_unique = 0;
+    // canonical order: stable LSD radix sort on (lo) then (hi). The unique
+    // count stays on the device (sd->n_contacts): the kernels below read it and
+    // their grids and buffers are sized for n_raw, so the host learns it only at
+    // the detection's final read-back.
     if (n_raw > 0) {
         raw_hi_s_.reserve(n_raw);
         raw_lo_s_.reserve(n_raw);
@@ -1194,14 +1206,11 @@ void World::detect(double query_radius, double radius, double relaxation, double
         k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, n_raw, uniq_flag_.ptr);
         CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw,
                                               stream_));
-        uint32_t last_flag = 0, last_pos = 0;
-        CC_CUDA(cudaMemcpyAsync(&last_flag, uniq_flag_.ptr + n_raw - 1, 4, cudaMemcpyDeviceToHost, stream_));
-        CC_CUDA(cudaMemcpyAsync(&last_pos, uniq_pos_.ptr + n_raw - 1, 4, cudaMemcpyDeviceToHost, stream_));
-        CC_CUDA(cudaStreamSynchronize(stream_));
-        n_unique = last_pos + last_flag;
-        c_kind_.reserve(n_unique);
-        c_verts_.reserve(n_unique);
-        c_eps_.reserve(n_unique);
+        k_unique_count<<<1, 1, 0, stream_>>>(uniq_flag_.ptr, uniq_pos_.ptr, n_raw, &sd->n_contacts);
+        ++launches_;
+        c_kind_.reserve(n_raw);
+        c_verts_.reserve(n_raw);
+        c_eps_.reserve(n_raw);
         k_compact<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_eps_.ptr,
                                                              uniq_flag_.ptr, uniq_pos_.ptr, n_raw, c_kind_.ptr,
                                                              c_verts_.ptr, c_eps_.ptr, nb);
@@ -1210,10 +1219,12 @@ void World::detect(double query_radius, double radius, double relaxation, double
     // incidence (moving vertices), active count, radii
     CC_CUDA(cudaMemsetAsync(inc_count_.ptr, 0, (moving_ + 1) * sizeof(uint32_t), stream_));
     CC_CUDA(cudaMemsetAsync(inc_cursor_.ptr, 0, (moving_ + 1) * sizeof(uint32_t), stream_));
-    if (n_unique > 0)
-        k_contact_finalize<<<grid_for(n_unique, 256), 256, 0, stream_>>>(view(), c_kind_.ptr, c_verts_.ptr, n_unique,
-                                                                         radius, inc_count_.ptr, &sd->active);
-    if (n_unique > 0) ++launches_;
+    if (n_raw > 0) {
+        k_contact_finalize<<<grid_for(n_raw, 256), 256, 0, stream_>>>(view(), c_kind_.ptr, c_verts_.ptr,
+                                                                      &sd->n_contacts, radius, inc_count_.ptr,
+                                                                      &sd->active);
+        ++launches_;
+    }
     {
         size_t need = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1), stream_);
@@ -1224,12 +1235,12 @@ void World::detect(double query_radius, double radius, double relaxation, double
         CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1),
                                               stream_));
     }
-    size_t n_inc_bound = 4 * n_unique;  // at most 4 moving vertices per contact
+    size_t n_inc_bound = 4 * n_raw;  // at most 4 moving vertices per contact
     inc_.reserve(std::max<size_t>(n_inc_bound, 1));
-    if (n_unique > 0) {
-        k_incidence_scatter<<<grid_for(n_unique, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
-                                                                           n_unique, inc_off_.ptr, inc_cursor_.ptr,
-                                                                           inc_.ptr);
+    if (n_raw > 0) {
+        k_incidence_scatter<<<grid_for(n_raw, 256), 256, 0, stream_>>>((uint32_t)moving_, c_kind_.ptr, c_verts_.ptr,
+                                                                        &sd->n_contacts, inc_off_.ptr, inc_cursor_.ptr,
+                                                                        inc_.ptr);
         k_incidence_sort_rows<<<grid_for(moving_, 256), 256, 0, stream_>>>((uint32_t)moving_, inc_off_.ptr, inc_.ptr);
         launches_ += 2;
     }
@@ -1241,7 +1252,6 @@ void World::detect(double query_radius, double radius, double relaxation, double
                             stream_));
     CC_CUDA(cudaGetLastError());
     sync_stats();
-    stats_h_.ptr->n_contacts = n_unique;
     stats_h_.ptr->n_incident &= 0xffffffffull;
     stats_h_.ptr->rebuild = rebuild ? 1 : 0;
     raise_device_error(stats_h_.ptr->error);

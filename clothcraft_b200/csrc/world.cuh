@@ -72,7 +72,7 @@ struct WorldView {
 struct DetectStats {  // read back after each detection
     unsigned long long n_vf, n_ee;             // candidate pairs (cache)
     unsigned long long n_raw;                  // raw contacts
-    unsigned long long n_contacts;             // unique (host-filled)
+    unsigned long long n_contacts;             // unique contacts
     unsigned long long active;
     unsigned long long vf_count, ee_count, rejections;
     unsigned long long min_dist_bits;
