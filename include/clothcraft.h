@@ -121,7 +121,14 @@ enum cc_init_mode {
  * row without a 5 % decrease of the residual while vertices are clipped to
  * their OGC balls, the next iteration starts with a refresh detection, as
  * the reference's refresh rule does once refresh_fraction * n vertices clip
- * (src/vbd.rs:326-334); 0 keeps the reference rule alone. */
+ * (src/vbd.rs:326-334); 0 keeps the reference rule alone.
+ * acceleration = rho in (0, 1): after every iteration the free vertices move
+ * to w_k (x_sweep - x_{k-2}) + x_{k-2}, clipped to their OGC balls, with the
+ * Chebyshev weights w_1 = 1, w_2 = 2/(2 - rho^2), w_k = 4/(4 - rho^2 w_{k-1})
+ * (Wang 2015). The sequence restarts at the step's start, at every refresh
+ * detection and after a residual evaluation that exceeds the previous one,
+ * so it is meant for use with residual_check_every > 0. 0 = off: the
+ * reference's iteration. */
 typedef struct cc_vbd_settings {
     double dt;
     uint32_t iterations;
