@@ -66,16 +66,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def sweep_traffic():
-    """DRAM bytes per k_sweep launch recorded from the committed ncu summary."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "k_sweep_sheet256_fold.md")) as f:
-            for line in f:
-                if line.startswith("traffic_bytes_per_launch:"):
-                    return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one k_sweep
+# launch on the fold, from one ncu capture of the profiling driver (the first
+# sweep launch of a 30-iteration step from the fold-phase state; cold cache,
+# since ncu flushes the caches between its passes):
+#   ncu --set full --clock-control none -k regex:k_sweep -s 0 -c 2 \
+#       python -m clothcraft_b200.profile_fold --steps 1 --lanes 1032 --fixed 30
+SWEEP_TRAFFIC_BYTES = 23094784.0
 
 
 def workload():
@@ -210,11 +207,13 @@ def step_settings(sc, mode, iterations=None, acceleration=ACCELERATION):
     return s.to_c()
 
 
-def cpu_reference_run(sc, state, steps, budget_s, threads, warmup=0):
+def cpu_reference_run(sc, state, steps, budget_s, threads, warmup=0, warmup_budget_s=None):
     """The reference CPU path (FP64 oracle restatement, all host threads) at
-    equal residual on the same workload from `state`: `warmup` untimed steps,
-    then up to `steps` timed steps or `budget_s`. Returns (done, seconds,
-    iterations of the timed steps, warm-up steps run)."""
+    equal residual on the same workload from `state`: up to `warmup` untimed
+    steps (within `warmup_budget_s`), then `steps` timed steps, stopping early
+    only once the timed steps have taken `budget_s`. Returns (done, seconds,
+    iterations and final relative force residuals of the timed steps, warm-up
+    steps run)."""
     import oracle
 
     o = oracle.Solver(sc, threads=threads)
@@ -223,19 +222,20 @@ def cpu_reference_run(sc, state, steps, budget_s, threads, warmup=0):
     t0 = time.perf_counter()
     warm = 0
     for _ in range(warmup):
-        if time.perf_counter() - t0 > budget_s / 2:
+        if warmup_budget_s is not None and time.perf_counter() - t0 > warmup_budget_s:
             break
         x, v, t, _ = o.step(x, v, t, st)
         warm += 1
-    done, its = 0, []
+    done, its, force = 0, [], []
     t1 = time.perf_counter()
     while done < steps:
         x, v, t, m = o.step(x, v, t, st)
         its.append(int(m["iterations"]))
+        force.append(m["relative_force_residual"])
         done += 1
-        if time.perf_counter() - t0 > budget_s:
+        if time.perf_counter() - t1 > budget_s:
             break
-    return done, time.perf_counter() - t1, its, warm
+    return done, time.perf_counter() - t1, (its, force), warm
 
 
 def run_reference(args, rank, world):
@@ -243,11 +243,14 @@ def run_reference(args, rank, world):
         return 0
     sc = workload()
     threads = os.cpu_count() or 1
-    budget = float(os.environ.get("CC_REFERENCE_BUDGET_S", "150"))
-    done, dt, its, warm = cpu_reference_run(sc, fold_state(), args.steps, budget, threads, warmup=args.warmup)
+    budget = float(os.environ.get("CC_REFERENCE_BUDGET_S", "480"))
+    warm_budget = float(os.environ.get("CC_REFERENCE_WARMUP_BUDGET_S", "45"))
+    done, dt, (its, force), warm = cpu_reference_run(sc, fold_state(), args.steps, budget, threads,
+                                                     warmup=args.warmup, warmup_budget_s=warm_budget)
     value = done / dt
-    sample = ("%d warm-up + %d timed steps from the fold-phase state at equal residual (bounded to ~%.0f s), "
-              "%d host threads, iterations %s" % (warm, done, budget, threads, its))
+    sample = ("%d warm-up + %d timed steps from the fold-phase state at equal residual (timed part bounded to "
+              "%.0f s, warm-up to %.0f s), %d host threads, iterations %s" % (warm, done, budget, warm_budget,
+                                                                              threads, its))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done, "warmup": warm,
         "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
@@ -256,6 +259,7 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "mean_iterations": float(np.mean(its)) if its else None,
+        "max_final_relative_force_residual": float(np.max(force)) if force else None,
         "note": "C++ FP64 restatement of the reference CPU path (VbdSolver::step + OgcWorld::detect, adaptive "
                 "init) run to the same residual target; the Rust original cannot be compiled in this "
                 "environment",
@@ -324,20 +328,31 @@ def main():
             s.step_resident(step_settings(sc, mode, iterations, acceleration))
         return s
 
-    def timed(solver, step_fn, k):
+    def timed(solver, step_fn, k, host_clock=False):
+        """Device time (CUDA events on the solver's stream) of k steps, or with
+        `host_clock` the host wall time of each blocking step call; the L2 flush
+        between steps runs outside the timed interval either way."""
         stream = torch.cuda.ExternalStream(L.cc_solver_stream(solver.h))
-        evs, metrics = [], []
+        evs, metrics, wall = [], [], 0.0
         for _ in range(k):
             with torch.cuda.stream(stream):
                 flush.zero_()
                 a = torch.cuda.Event(enable_timing=True)
                 b = torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-            metrics.append(step_fn())
+            if host_clock:
+                torch.cuda.synchronize()
+                h0 = time.perf_counter()
+                metrics.append(step_fn())
+                wall += time.perf_counter() - h0
+            else:
+                metrics.append(step_fn())
             with torch.cuda.stream(stream):
                 b.record(stream)
             evs.append((a, b))
         torch.cuda.synchronize()
+        if host_clock:
+            return 1000.0 * wall, metrics
         return sum(a.elapsed_time(b) for a, b in evs), metrics
 
     def max_over_ranks(ms):
@@ -347,11 +362,11 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         return float(tt.item())
 
-    def leg(solver, step_fn, k):
+    def leg(solver, step_fn, k, host_clock=False):
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        ms, mets = timed(solver, step_fn, k)
+        ms, mets = timed(solver, step_fn, k, host_clock)
         if dist:
             dist.barrier()
         return max_over_ranks(ms), mets
@@ -361,10 +376,14 @@ def main():
     learned = make(1)
     tuned["lanes"] = int(L.cc_solver_get_lanes(learned.h))
     plain = make(0)
-    warm_learned = learned.get_state()
+    warm_state = learned.get_state()
     clocks = ClockSampler(local).__enter__()
-    # ---- value: learned init at equal residual, device-resident
+    # ---- value: learned init at equal residual, device-resident; the colour
+    # sweeps of every iteration are bracketed by one event pair (the roofline's
+    # launch durations and the breakdown come from this same timed leg)
+    L.cc_solver_set_profiling(learned.h, 1)
     t_l, mets_l = leg(learned, lambda: learned.step_resident(st_l), K)
+    L.cc_solver_set_profiling(learned.h, 0)
     # ---- plain adaptive init at equal residual
     t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
     # ---- both inits without acceleration (the reference's iteration)
@@ -386,12 +405,7 @@ def main():
         state["t"], m = e2e_solver.step_into(xh, vh, state["t"], st_l)
         return m
 
-    t_e2e, mets_e2e = leg(e2e_solver, host_step, K)
-    # ---- per-launch sweep timing for the roofline (learned, same start)
-    learned.set_state(*warm_learned)
-    L.cc_solver_set_profiling(learned.h, 1)
-    _, mets_prof = leg(learned, lambda: learned.step_resident(st_l), K)
-    L.cc_solver_set_profiling(learned.h, 0)
+    t_e2e, mets_e2e = leg(e2e_solver, host_step, K, host_clock=True)
     # ---- the reference's fixed-iteration step (plain init, 30 iterations), for context
     st_f = step_settings(sc, 0, FIXED_ITERATIONS)
     st_f.residual_check_every = FIXED_ITERATIONS  # one residual evaluation, after the last iteration
@@ -420,24 +434,38 @@ def main():
                 "mean_iterations": float(np.mean(its)), "median_iterations": float(np.median(its)),
                 "capped_fraction": float(np.mean(np.array(its) >= ITERATION_CAP)),
                 "mean_final_relative_residual": float(np.mean([m["relative_residual"] for m in mets])),
-                "max_final_relative_residual": float(np.max([m["relative_residual"] for m in mets]))}
+                "max_final_relative_residual": float(np.max([m["relative_residual"] for m in mets])),
+                "mean_final_relative_force_residual": float(np.mean([m["relative_force_residual"]
+                                                                     for m in mets])),
+                "max_final_relative_force_residual": float(np.max([m["relative_force_residual"]
+                                                                   for m in mets]))}
 
     # ---- roofline of the dominant kernel (colour sweep), learned leg
     peak, peak_kind = load_peaks()
     static_b = static_bytes_per_sweep(sc)
-    sweep_ms = sum(m["sweep_ms"] for m in mets_prof)
-    sweeps = sum(m["sweep_launches"] for m in mets_prof)
-    alg_bytes = sum((static_b + 28.0 * m["contact_incidence"]) * m["iterations"] for m in mets_prof)
+    sweep_ms = sum(m["sweep_ms"] for m in mets_l)
+    sweeps = sum(m["sweep_launches"] for m in mets_l)
+    alg_bytes = sum((static_b + 28.0 * m["contact_incidence"]) * m["iterations"] for m in mets_l)
     achieved = alg_bytes / (sweep_ms / 1000.0) / 1e9 if sweep_ms > 0 else None
+    det_ms = sum(m["detection_ms"] for m in mets_l) / K
+    col_ms = sum(m["color_ms"] for m in mets_l) / K
+    init_ms = sum(m["init_ms"] for m in mets_l) / K
+    breakdown = {"detection": det_ms, "coloring": col_ms, "learned_guess": init_ms, "sweeps": sweep_ms / K,
+                 "other": t_l / K - det_ms - col_ms - init_ms - sweep_ms / K,
+                 "note": "from the timed learned leg: detection and colouring by host clock (they end in a "
+                         "device sync), learned guess and sweeps by CUDA events; other = ms_per_step minus "
+                         "the four (predict, warm start, residual checks, acceleration, commit, metrics)"}
 
-    # ---- CPU baseline (rank 0, N=1 only): the oracle at equal residual
+    # ---- CPU baseline (rank 0, N=1 only): the oracle at equal residual from
+    # the state the timed legs start from, a sample of about 30 s
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        done, dt, its_cpu, _ = cpu_reference_run(sc, start, 3, 25.0, threads)
+        done, dt, (its_cpu, _), _ = cpu_reference_run(sc, warm_state, 8, 30.0, threads)
         cpu = {"value": done / dt, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": "first %d step(s) from the fold-phase state at equal residual (iterations %s), FP64 "
-                         "oracle restatement of the reference CPU path, %d threads" % (done, its_cpu, threads)}
+               "sample": "%d step(s) from the state after the warm-up at equal residual (iterations %s, about "
+                         "30 s), FP64 oracle restatement of the reference CPU path, %d threads" % (
+                             done, its_cpu, threads)}
 
     if dist:
         dist.barrier()
@@ -480,28 +508,25 @@ def main():
             "peak": peak,
             "unit": "GB/s",
             "frac": (achieved / peak) if achieved else None,
-            "traffic": sweep_traffic(),
-            "traffic_note": "dram read+write bytes per k_sweep launch from one ncu capture "
-                            "(profiles/k_sweep_sheet256_fold.md, cold cache)",
+            "traffic": SWEEP_TRAFFIC_BYTES,
+            "traffic_note": "dram read+write bytes per k_sweep launch, one ncu capture on the fold (cold cache)",
             "peak_kind": peak_kind,
             "sweep_launches": int(sweeps),
             "avg_launch_us": 1000.0 * sweep_ms / max(sweeps, 1),
+            "launch_timing": "CUDA events around each iteration's back-to-back colour sweeps in the timed "
+                             "learned leg, divided by the launches",
             "algorithmic_bytes_per_launch": alg_bytes / max(sweeps, 1),
-            "sweep_share_of_step": sweep_ms / max(sum(m["gpu_compute_ms"] for m in mets_prof), 1e-9),
+            "sweep_share_of_step": sweep_ms / t_l,
         },
         "cpu_baseline": cpu,
         "e2e": {"value": world * K / (t_e2e / 1000.0), "unit": UNIT, "h2d_bytes_per_step": 2 * sc.n * 24,
                 "d2h_bytes_per_step": 2 * sc.n * 24, "mean_iterations": float(np.mean(iters(mets_e2e))),
+                "timing": "host clock around each blocking VbdSolver.step_into call",
                 "host_memory": "pinned, [n][3] float64 x and v, stepped in place (VbdSolver.step_into)"},
         "gpu_launches": int(sum(m["kernel_launches"] for m in mets_l)),
         "lanes_per_vertex": int(L.cc_solver_get_lanes(learned.h)) & 0xff,
         "blocks_per_sm_cap": int(L.cc_solver_get_lanes(learned.h)) >> 8,
-        "breakdown_ms_per_step": {
-            "detection": sum(m["detection_ms"] for m in mets_l) / K,
-            "coloring": sum(m["color_ms"] for m in mets_l) / K,
-            "learned_guess": sum(m["init_ms"] for m in mets_l) / K,
-            "sweeps": sweep_ms / K,
-        },
+        "breakdown_ms_per_step": breakdown,
         "clocks": clocks.summary(),
         "detections_per_step": sum(m["detection_updates"] for m in mets_l) / K,
         "contact_terms_last": mets_l[-1]["contact_terms"] if mets_l else None,

@@ -113,13 +113,13 @@ class cc_metrics(C.Structure):
         ("relative_residual", C.c_double), ("initial_relative_residual", C.c_double),
         ("has_relative_residual", C.c_int32), ("init_used", C.c_int32),
         ("init_energy_adaptive", C.c_double), ("init_energy_learned", C.c_double),
-        ("init_ms", C.c_double)]
+        ("init_ms", C.c_double), ("relative_force_residual", C.c_double)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved0"}
         d["residual_rms_n"] = d["residual_rms_n"] if d.pop("has_residual") else None
         if not d.pop("has_relative_residual"):
-            d["relative_residual"] = d["initial_relative_residual"] = None
+            d["relative_residual"] = d["initial_relative_residual"] = d["relative_force_residual"] = None
         return d
 
 

@@ -210,10 +210,7 @@ void Coloring::compute(const ColorView& view, cudaStream_t s) {
     CC_CUDA(cudaMemsetAsync(changed_.ptr + 2, 0xff, sizeof(unsigned int), s));
     k_color_probe<<<grid_for(n, 256), 256, 0, s>>>(view, cur_, changed_.ptr + 2);
     size_t smem = n <= kSmemColors ? n * sizeof(uint16_t) : 0;
-    if (smem > 48 * 1024 && !smem_attr_)
-        CC_CUDA(cudaFuncSetAttribute(k_color_chunked, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(kSmemColors * sizeof(uint16_t))));
-    smem_attr_ = true;
+    allow_dynamic_smem(k_color_chunked, smem);
     k_color_chunked<<<1, kChunk, smem, s>>>(view, cur_, changed_.ptr + 2, changed_.ptr, changed_.ptr + 1);
     launches_ += 2;
     CC_CUDA(cudaGetLastError());

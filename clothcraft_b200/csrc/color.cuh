@@ -43,7 +43,6 @@ class Coloring {
     uint32_t n_colors_ = 0;
     size_t last_iterations_ = 0;
     uint64_t launches_ = 0;
-    bool smem_attr_ = false;
 };
 
 }  // namespace cc

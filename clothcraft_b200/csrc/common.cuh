@@ -140,6 +140,16 @@ __host__ __device__ inline double from_order_key(unsigned long long k) {
     return d;
 }
 
+// CUDA keeps a kernel's dynamic shared-memory limit per device, so the limit
+// is raised before every launch that needs more than 48 KB (a host call of a
+// few microseconds) instead of once per process: a process that switches
+// devices with cc_set_device then finds it raised on each device it uses.
+template <class K>
+inline void allow_dynamic_smem(K* kernel, size_t bytes) {
+    if (bytes > 48 * 1024)
+        CC_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 inline int grid_for(size_t n, int block) {
     size_t g = (n + block - 1) / block;
     if (g < 1) g = 1;

@@ -1379,6 +1379,10 @@ void World::download(std::vector<uint32_t>& kind, std::vector<uint32_t>& verts, 
 // the process exits. Every call shares it and it keeps the previous call's
 // contents, so each call clears what must start from a known value, and two
 // calls whose kernels overlap on the GPU (e.g. on different streams) race.
+// Calls made through this entry point from several host threads are
+// serialised by a mutex held from the first launch to the read-back, so
+// their launches cannot interleave; kernels that another process or another
+// copy of the library runs on the same array are outside its reach.
 namespace cc {
 
 constexpr uint64_t kNoAllocMaxVertices = 262144;
@@ -1512,18 +1516,19 @@ extern "C" int32_t cc_ogc_radii_noalloc(const double* x, uint64_t n_all, uint64_
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
         return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: no current CUDA device");
-    unsigned long long* scratch;
-    {
+    // one call at a time in this process: the launches and the read-back of
+    // two host threads must not interleave on the shared scratch array
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    // an earlier, unrelated launch error is not this call's failure
+    (void)cudaGetLastError();
+    if (!g_noalloc_address[dev]) {
         // once per device, with that device current: the symbol's device address
-        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_address[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
-                return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: scratch address unavailable");
-            g_noalloc_address[dev] = static_cast<unsigned long long*>(p);
-        }
-        scratch = g_noalloc_address[dev];
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
+            return record_global_error(CC_ERR_CUDA, "cc_ogc_radii_noalloc: scratch address unavailable");
+        g_noalloc_address[dev] = static_cast<unsigned long long*>(p);
     }
+    unsigned long long* scratch = g_noalloc_address[dev];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     NoAllocArgs a{x, (uint32_t)n_all, (uint32_t)moving, (uint32_t)n_triangles, (uint32_t)n_edges, triangles, edges,
                   vf_pairs, ee_pairs, n_vf, n_ee, query_radius, relaxation, scratch};

@@ -466,11 +466,7 @@ void Mlp::forward(const float* features, uint64_t n, float* out, int precision, 
         return;
     }
     size_t smem = (kMlpParams + 1 + kMlpHidden * kFwdBlock) * sizeof(float);
-    static bool attr = false;
-    if (!attr) {
-        CC_CUDA(cudaFuncSetAttribute(k_mlp_forward_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    allow_dynamic_smem(k_mlp_forward_f32, smem);
     uint64_t blocks = (n + kFwdBlock - 1) / kFwdBlock;
     unsigned grid = (unsigned)std::min<uint64_t>(blocks, 148ull * 4ull);
     k_mlp_forward_f32<<<grid, kFwdBlock, smem, st>>>(p_.ptr, features, n, out);
@@ -481,11 +477,7 @@ void Mlp::gradients(const float* features, const float* targets, const uint32_t*
                     float* loss, cudaStream_t st) {
     if (n == 0) throw Failure{CC_ERR_INVALID_ARGUMENT, "MLP gradients need at least one sample"};
     size_t smem = (size_t)kTrainFloats * sizeof(float);
-    static bool attr = false;
-    if (!attr) {
-        CC_CUDA(cudaFuncSetAttribute(k_mlp_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr = true;
-    }
+    allow_dynamic_smem(k_mlp_train_tile, smem);
     uint64_t tiles = (n + kTile - 1) / kTile;
     int rows = (int)std::min<uint64_t>(tiles, 148ull);
     partial_.reserve((size_t)rows * (kMlpParams + 1));

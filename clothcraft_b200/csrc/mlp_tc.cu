@@ -212,7 +212,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float* __restri
         if (!mbar_wait_bounded(barrier, phase, kWaitNs)) {
             failed = true;
             // the MMAs of this layer may still be in flight: give them one more
-            // bounded wait before the TMEM is released
+            // bounded wait before the TMEM is released. A layer is at most four
+            // K=16 MMAs on a 128x64 tile (microseconds of tensor work), so a
+            // commit that has not arrived after 0.6 s was never going to; the
+            // columns are still freed because a CTA must not exit holding TMEM.
             mbar_wait_bounded(barrier, phase, kWaitNs / 5);
         }
         phase ^= 1u;
@@ -301,11 +304,7 @@ void Mlp::forward_tc(const float* features, uint64_t n, float* out, cudaStream_t
     refresh_half(st);
     err_.reserve(1);
     CC_CUDA(cudaMemsetAsync(err_.ptr, 0, sizeof(unsigned int), st));
-    static bool attr = false;
-    if (!attr) {
-        CC_CUDA(cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmRequest));
-        attr = true;
-    }
+    allow_dynamic_smem(k_mlp_forward_tc, kSmRequest);
     uint64_t tiles = (n + kTcM - 1) / kTcM;
     unsigned grid = (unsigned)std::min<uint64_t>(tiles, 148ull * 2ull);
     k_mlp_forward_tc<<<grid, 128, kSmRequest, st>>>(p_.ptr, reinterpret_cast<const unsigned char*>(w16_.ptr), features,

@@ -82,6 +82,7 @@ struct StepScalars {
     double gy2;        // |grad E(y)|^2, y the inertial target
     double gx2;        // |grad E(x)|^2 at the last evaluation
     double gx2_init;   // |grad E|^2 of the initial guess
+    double gx2_plain;  // |grad E(x)|^2 after the last iteration, unprojected
     double e_init[2];  // step energy of the adaptive / full-scale learned guess
     int init_used;
     double gx2_iter[256];   // |P grad E(x)|^2 after iteration it (evaluated ones)
@@ -842,24 +843,26 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
             for (uint32_t it = c0; it < c1; ++it) {
                 sv.iteration = it;
                 sv.clipped = &sc.ptr->clipped_iter[it];
+                // profiling: one event pair around the iteration's back-to-back
+                // colour sweeps (nothing else is enqueued between them)
+                if (profiling) {
+                    while (prof_events.size() < prof_used + 2) {
+                        cudaEvent_t e;
+                        CC_CUDA(cudaEventCreate(&e));
+                        prof_events.push_back(e);
+                    }
+                    CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
+                }
                 for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
                     uint32_t cnt = off[c + 1] - off[c];
                     if (cnt == 0) continue;
-                    if (profiling) {
-                        while (prof_events.size() < prof_used + 2) {
-                            cudaEvent_t e;
-                            CC_CUDA(cudaEventCreate(&e));
-                            prof_events.push_back(e);
-                        }
-                        CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
-                    }
                     launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
-                    if (profiling) {
-                        CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
-                        prof_pairs.push_back({prof_used, it});
-                        prof_used += 2;
-                    }
                     ++own_launches;
+                }
+                if (profiling) {
+                    CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
+                    prof_pairs.push_back({prof_used, it});
+                    prof_used += 2;
                 }
                 k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold, rho2);
                 if (accelerate) {
@@ -905,6 +908,11 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
             it0 = s.iterations;
         }
     }
+    if (checks) {
+        // the plain force norm of the final iterate with the OGC terms in force
+        grad_sq_into(sweep_view(cv, s, grab), &sc.ptr->gx2_plain, false);
+        CC_CUDA(cudaGetLastError());
+    }
     for (uint32_t it = 0; it < executed; ++it) m.truncated_vertices += sc_h.ptr->clipped_iter[it];
     m.iterations = executed;
     m.vertex_solves = (uint64_t)n_free * executed;
@@ -931,6 +939,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     CC_CUDA(cudaGetLastError());
     read_scalars();
     if (sc_h.ptr->error & DERR_NONFINITE_RESULT) throw Failure{CC_ERR_NON_FINITE, "Non-finite VBD result; state unchanged"};
+    if (checks) m.relative_force_residual = std::sqrt(sc_h.ptr->gx2_plain / sc_h.ptr->gy2);
     if (sc_h.ptr->error & DERR_TRUST_REGION) throw Failure{CC_ERR_CONTACT, "OGC trust-region invariant failed"};
     m.residual_rms_n = std::sqrt(sc_h.ptr->residual / (double)(3 * (size_t)n));
     m.has_residual = 1;

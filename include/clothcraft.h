@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define CC_ABI_VERSION 2
+#define CC_ABI_VERSION 3
 
 enum cc_status {
     CC_OK = 0,
@@ -183,6 +183,10 @@ typedef struct cc_metrics {
     double init_energy_learned;     /* of the full-scale learned guess        */
                                     /* (learned mode; NaN otherwise)          */
     double init_ms;                 /* device time of the learned guess       */
+    /* the plain force norm ||grad E(x)|| / ||grad E(y)|| after the last
+     * iteration (no projection P; the same E, y and OGC terms as
+     * relative_residual), defined when has_relative_residual = 1 */
+    double relative_force_residual;
 } cc_metrics;
 
 /* ContactSet (src/ogc/world.rs:73-107) in caller-owned arrays. The contact
@@ -270,8 +274,9 @@ uint64_t cc_solver_total(const cc_solver* solver);
  * (the wgpu backend times its compute pass with timestamp queries,
  * src/gpu_vbd/cache.rs:16-33). */
 void* cc_solver_stream(const cc_solver* solver);
-/* When enabled, each colour-sweep launch is bracketed by CUDA events and
- * cc_metrics.sweep_ms reports their summed device time. */
+/* When enabled, each iteration's colour sweeps (launched back to back) are
+ * bracketed by one pair of CUDA events and cc_metrics.sweep_ms reports their
+ * summed device time over the iterations the step ran. */
 int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
 /* Threads that cooperate on one vertex's local solve (1, 2, 4, 8, 16 or 32),
  * optionally | (cap << 8) with cap = 3, 4, 5, 6 or 8 resident 128-thread
@@ -416,7 +421,9 @@ int32_t cc_solver_step_sample(cc_solver* solver, const cc_vbd_settings* settings
  * returns after they finish. The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) with that device current;
  * make that first call before any stream capture. All calls share the one
- * array, so calls whose kernels overlap on the GPU race. */
+ * array, so calls whose kernels overlap on the GPU race. Calls from several
+ * host threads of one process are serialised inside the library (a mutex
+ * held from the first launch until the call's kernels have finished). */
 int32_t cc_ogc_radii_noalloc(const double* x, uint64_t n_all, uint64_t moving, const uint32_t* triangles,
                              uint64_t n_triangles, const uint32_t* edges, uint64_t n_edges,
                              const uint32_t* vf_pairs, uint64_t n_vf, const uint32_t* ee_pairs, uint64_t n_ee,

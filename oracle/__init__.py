@@ -47,6 +47,7 @@ def lib():
             "or_solver_world": (vp, [vp]),
             "or_solver_step": (C.c_int32, [vp, c_double_p, c_double_p, c_double_p, C.POINTER(cc_vbd_settings),
                                            C.POINTER(cc_grab), C.POINTER(cc_metrics)]),
+            "or_solver_set_learned_correction": (C.c_int32, [vp, C.POINTER(C.c_float), C.c_uint64]),
             "or_solver_colors": (C.c_int32, [vp, c_double_p, C.c_double, C.POINTER(cc_ogc_settings),
                                              C.POINTER(cc_grab), c_uint32_p, c_uint32_p]),
             "or_solver_local_blocks": (C.c_int32, [vp, c_double_p, C.c_double, C.POINTER(cc_vbd_settings),
@@ -274,6 +275,14 @@ class Solver:
         if rc != 0:
             raise self._err(rc)
         return x, v, t.value, m.as_dict()
+
+    def set_learned_correction(self, corr):
+        """Network output ([free vertices, 3] float32, vertex order) that the
+        next step with init_mode = 1 turns into the library's learned guess."""
+        c = np.ascontiguousarray(corr, dtype=np.float32).reshape(-1, 3)
+        rc = lib().or_solver_set_learned_correction(self.h, c.ctypes.data_as(C.POINTER(C.c_float)), c.shape[0])
+        if rc != 0:
+            raise self._err(rc)
 
     def newton_step(self, x_old, v_old, settings: cc_vbd_settings, newton_iterations=30, pcg_iterations=250,
                     abs_tol=1e-6, rel_tol=1e-4, threads=8):

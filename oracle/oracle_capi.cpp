@@ -58,6 +58,7 @@ VbdSettings to_vbd(const cc_vbd_settings* s) {
     o.residual_check_every = s->residual_check_every;
     o.stall_refresh = s->stall_refresh;
     o.acceleration = s->acceleration;
+    o.init_mode = (int)s->init_mode;
     return o;
 }
 
@@ -153,6 +154,8 @@ void fill_metrics(const VbdMetrics& m, cc_metrics* out) {
     out->has_relative_residual = m.has_relative_residual ? 1 : 0;
     out->relative_residual = m.relative_residual;
     out->initial_relative_residual = m.initial_relative_residual;
+    out->relative_force_residual = m.relative_force_residual;
+    out->init_used = m.init_used ? 1 : 0;
 }
 
 int fill_contacts(const ContactSet& cs, size_t moving, cc_contacts* out) {
@@ -271,6 +274,23 @@ void or_solver_destroy(or_solver* s) { delete s; }
 uint64_t or_solver_moving(const or_solver* s) { return s->s.mesh.n; }
 uint64_t or_solver_total(const or_solver* s) { return s->s.world.topology.neighbors.size(); }
 or_world* or_solver_world(or_solver* s) { return &s->world_view; }
+
+// Correction (rows = free vertices in vertex order, [rows][3] float, the
+// layout of the library's network output) for the next learned-init step.
+int32_t or_solver_set_learned_correction(or_solver* s, const float* corr, uint64_t rows) {
+    size_t n = s->s.mesh.n;
+    size_t free_rows = 0;
+    for (size_t i = 0; i < n; ++i) free_rows += s->s.mesh.pinned[i] ? 0 : 1;
+    if (rows != free_rows) return s->fail(Error{1, "correction rows must equal the free vertices"});
+    s->s.learned_correction.assign(n, D3{0, 0, 0});
+    size_t r = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (s->s.mesh.pinned[i]) continue;
+        s->s.learned_correction[i] = D3{(double)corr[3 * r], (double)corr[3 * r + 1], (double)corr[3 * r + 2]};
+        ++r;
+    }
+    return CC_OK;
+}
 
 int32_t or_solver_step(or_solver* s, double* x, double* v, double* time, const cc_vbd_settings* settings,
                        const cc_grab* grab, cc_metrics* metrics) {

@@ -230,6 +230,41 @@ double VbdSolver::grad_sq(const std::vector<D3>& x, const ContactSet& contacts, 
     return s;
 }
 
+double VbdSolver::step_energy(const std::vector<D3>& x, const ContactSet& contacts, const std::vector<D3>& target,
+                              const std::vector<double>& inertia, const VbdSettings& settings,
+                              const Grab* grab) const {
+    const size_t n = mesh.n;
+    double e = 0.0;
+    for (size_t v = 0; v < n; ++v)
+        if (!mesh.pinned[v]) e += 0.5 * inertia[v] * length_squared(x[v] - target[v]);
+    for (const Triangle& t : mesh.triangles) {
+        V3<double> q[3] = {lift<double>(x[t.vertices[0]]), lift<double>(x[t.vertices[1]]),
+                           lift<double>(x[t.vertices[2]])};
+        e += membrane<double>(q, t.inv_dm, t.area, mesh.materials[t.material]);
+    }
+    for (const Hinge& h : mesh.hinges) {
+        V3<double> q[4] = {lift<double>(x[h.vertices[0]]), lift<double>(x[h.vertices[1]]),
+                           lift<double>(x[h.vertices[2]]), lift<double>(x[h.vertices[3]])};
+        e += bending<double>(q, h.weight, h.across, mesh.materials[h.material]);
+    }
+    for (const Stitch& st : mesh.stitches) {
+        D3 d{0, 0, 0};
+        for (const auto& [j, w] : st.terms) d = d + x[j] * w;
+        e += 0.5 * st.stiffness * length_squared(d);
+    }
+    for (const Contact& c : contacts.contacts) {
+        V3<double> q[4] = {lift<double>(x[c.vertices[0]]), lift<double>(x[c.vertices[1]]),
+                           lift<double>(x[c.vertices[2]]), lift<double>(x[c.vertices[3]])};
+        e += contact_energy<double>(c, q, settings.contact.radius, settings.contact.stiffness);
+    }
+    if (grab) {
+        D3 d = grab->target * -1.0;
+        for (int j = 0; j < 3; ++j) d = d + x[grab->vertices[j]] * grab->weights[j];
+        e += 0.5 * grab->stiffness * length_squared(d);
+    }
+    return e;
+}
+
 VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab* grab) {
     if (!settings.valid()) throw Error{1, "Invalid VBD settings"};
     const size_t n = mesh.n;
@@ -285,6 +320,42 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
             bool b;
             x[i] = contacts.truncate(i, guess[i], b);
             clipped += b ? 1 : 0;
+        }
+    }
+    if (settings.init_mode == 1) {
+        // The library's learned guess (clothcraft_b200/csrc/solver.cu,
+        // learned_guess): candidates guess + a u c for a = 1, 1/2, 1/4, each
+        // clipped to the OGC balls; the lowest step energy replaces the
+        // adaptive warm start only if it is strictly lower.
+        if (learned_correction.size() != n)
+            throw Error{1, "learned initial guess requested but no correction was given"};
+        double gl = length(settings.gravity);
+        double unit = gl * dt * dt > 1e-9 ? gl * dt * dt : 1e-3;
+        double best_e = step_energy(x, contacts, target, inertia, settings, grab);
+        std::vector<D3> best;
+        size_t clipped_best = clipped;
+        for (double a : {1.0, 0.5, 0.25}) {
+            std::vector<D3> cand = x;
+            size_t cnt = 0;
+            for (size_t i = 0; i < n; ++i) {
+                if (mesh.pinned[i]) continue;
+                D3 p = guess[i] + learned_correction[i] * (unit * a);
+                if (!finite(p)) p = guess[i];
+                bool b;
+                cand[i] = contacts.truncate(i, p, b);
+                cnt += b ? 1 : 0;
+            }
+            double e = step_energy(cand, contacts, target, inertia, settings, grab);
+            if (e < best_e) {
+                best_e = e;
+                best.swap(cand);
+                clipped_best = cnt;
+                metrics.init_used = true;
+            }
+        }
+        if (metrics.init_used) {
+            x.swap(best);
+            clipped = clipped_best;
         }
     }
     const bool checks = settings.residual_check_every > 0 || settings.residual_tolerance > 0.0;
@@ -421,6 +492,9 @@ VbdMetrics VbdSolver::step(State& state, const VbdSettings& settings, const Grab
             }
         }
     }
+    if (checks)  // the plain force norm of the final iterate, OGC terms in force
+        metrics.relative_force_residual =
+            std::sqrt(grad_sq(x, contacts, target, inertia, settings, grab, false) / gy2);
     for (const auto& p : x)
         if (!finite(p)) throw Error{4, "Non-finite VBD result; state unchanged"};
     for (size_t i = 0; i < n; ++i)

@@ -51,6 +51,9 @@ struct VbdSettings {  // src/vbd.rs:18-52
     // Extension: Chebyshev semi-iterative acceleration of the sweeps with
     // spectral-radius estimate rho in [0, 1) (0 = off, the reference).
     double acceleration = 0.0;
+    // Extension: 1 = start from the library's learned guess (the correction
+    // of the adaptive guess is given, see VbdSolver::learned_correction).
+    int init_mode = 0;
     bool valid() const;
 };
 
@@ -72,6 +75,8 @@ struct VbdMetrics {  // src/vbd.rs:61-83
     double residual_rms_n = 0;
     bool has_relative_residual = false;
     double relative_residual = 0, initial_relative_residual = 0;
+    double relative_force_residual = 0;  // unprojected, after the last iteration
+    bool init_used = false;               // the learned guess replaced the adaptive one
 };
 
 struct State {
@@ -94,6 +99,11 @@ struct Prediction {  // src/vbd/prediction.rs:6-54
 struct VbdSolver {  // src/vbd.rs:89-99
     Prediction prediction;
     std::vector<D3> last_guess;  // adaptive guess of the last step (learned-guess feature)
+    // Network output of the next learned-init step: per moving vertex the
+    // correction c of the adaptive guess, in units of |g| dt^2 (pinned rows
+    // unused). The network itself is checked separately; the step restates
+    // what the library does with its output.
+    std::vector<D3> learned_correction;
     Mesh mesh;
     OgcWorld world;
     std::vector<std::vector<uint32_t>> triangles, hinges, vertex_stitches, graph;
@@ -111,6 +121,11 @@ struct VbdSolver {  // src/vbd.rs:89-99
     double grad_sq(const std::vector<D3>& x, const ContactSet& contacts, const std::vector<D3>& target,
                    const std::vector<double>& inertia, const VbdSettings& settings, const Grab* grab,
                    bool project) const;
+    // step objective at positions x (all vertices): inertia of the free
+    // vertices plus every triangle, hinge, stitch, contact term and the grab
+    // once each (the library's k_term_energy items)
+    double step_energy(const std::vector<D3>& x, const ContactSet& contacts, const std::vector<D3>& target,
+                       const std::vector<double>& inertia, const VbdSettings& settings, const Grab* grab) const;
 };
 
 // src/vbd/coloring.rs:5-43

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_entry_point():
 
 def test_abi_version_and_no_device_is_reported_not_faked():
     L = native.load()
-    assert L.cc_abi_version() == 2
+    assert L.cc_abi_version() == 3
     count = C.c_int()
     try:
         import torch

@@ -39,6 +39,6 @@ def test_header_compiles_as_c99_and_links(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
     version, *sizes = [int(t) for t in out.stdout.split()]
-    assert version == 2
+    assert version == 3
     assert sizes == [C.sizeof(abi.cc_vbd_settings), C.sizeof(abi.cc_metrics), C.sizeof(abi.cc_grab),
                      C.sizeof(abi.cc_material), C.sizeof(abi.cc_ogc_settings), C.sizeof(abi.cc_contacts)]

@@ -33,11 +33,13 @@ def test_config_names_the_workload_and_its_target():
     assert "flushed" in c["l2"]
 
 
-def test_roofline_traffic_is_read_from_the_committed_summary():
-    t = bench.sweep_traffic()
-    assert t is not None and 1e6 < t < 1e9
-    with open(os.path.join(bench.ROOT, "profiles", "k_sweep_sheet256_fold.md")) as f:
-        assert any(line.startswith("traffic_bytes_per_launch: %d" % int(t)) for line in f)
+def test_roofline_traffic_is_a_recorded_constant():
+    """The sweep's DRAM bytes per launch are a constant recorded beside the ncu
+    command that measured them; bench.py reads no file for them."""
+    t = bench.SWEEP_TRAFFIC_BYTES
+    assert 1e6 < t < 1e9
+    src = open(os.path.join(bench.ROOT, "bench.py")).read()
+    assert "profiles/" not in src and "ncu --set full --clock-control none -k regex:k_sweep" in src
 
 
 def test_cpu_reference_arm_runs_the_reference_iteration(monkeypatch):
@@ -53,11 +55,30 @@ def test_cpu_reference_arm_runs_the_reference_iteration(monkeypatch):
 
         def step(self, x, v, t, st):
             seen.append((st.init_mode, st.acceleration, st.residual_tolerance, st.iterations, self.threads))
-            return x, v, t + st.dt, {"iterations": 7}
+            return x, v, t + st.dt, {"iterations": 7, "relative_force_residual": 1e-3}
 
     monkeypatch.setattr(oracle, "Solver", FakeSolver)
     sc = bench.workload()
     state = (sc.x0, sc.v0, 0.0)
-    done, dt, its, warm = bench.cpu_reference_run(sc, state, 2, 60.0, 3, warmup=1)
-    assert done == 2 and warm == 1 and its == [7, 7] and dt >= 0.0
+    done, dt, (its, force), warm = bench.cpu_reference_run(sc, state, 2, 60.0, 3, warmup=1)
+    assert done == 2 and warm == 1 and its == [7, 7] and force == [1e-3, 1e-3] and dt >= 0.0
     assert seen == [(0, 0.0, bench.TOLERANCE, bench.ITERATION_CAP, 3)] * 3
+
+
+def test_cpu_reference_arm_runs_every_timed_step_within_its_budget(monkeypatch):
+    """The reference arm times all K steps unless they outlast the budget;
+    the warm-up has a budget of its own."""
+    import oracle
+
+    class FakeSolver:
+        def __init__(self, scene, threads=1):
+            pass
+
+        def step(self, x, v, t, st):
+            return x, v, t + st.dt, {"iterations": 3, "relative_force_residual": 1e-3}
+
+    monkeypatch.setattr(oracle, "Solver", FakeSolver)
+    sc = bench.workload()
+    done, _, (its, _), warm = bench.cpu_reference_run(sc, (sc.x0, sc.v0, 0.0), 20, 1e6, 1, warmup=5,
+                                                      warmup_budget_s=1e6)
+    assert done == 20 and warm == 5 and len(its) == 20

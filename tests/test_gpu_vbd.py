@@ -170,6 +170,31 @@ def test_many_steps_energy_and_residual_within_one_percent():
     assert abs(eg - eo) <= RELATIVE_TOL * abs(eo), (eg, eo)
 
 
+def test_config0_hundred_steps_energy_and_residual_within_one_percent():
+    """Bar (b) on config 0 (64x64 sheet, two pinned corners, r = 0.1 m
+    icosphere, 20 iterations): after 100 steps of each side's own trajectory
+    the potential energy, the reference's residual_rms_n and the relative
+    force residual agree within 1 %. The residual is evaluated once, after the
+    last iteration of every step, which does not change the iterates."""
+    sc = scenes.config0()
+    s = sc.settings
+    s.residual_check_every = s.iterations
+    out, g, o = run_both(sc, 100, s)
+    xg, xo, mg, mo = out[-1]
+    assert mg["contact_terms"] > 0 and mo["contact_terms"] > 0  # draped over the sphere by then
+    for key in ("residual_rms_n", "relative_force_residual", "relative_residual"):
+        assert abs(mg[key] - mo[key]) <= RELATIVE_TOL * abs(mo[key]), (key, mg[key], mo[key])
+    st = s.to_c()
+    grav = np.array(st.gravity)
+
+    def potential(x):  # elastic + contact (oracle blocks, each term per incident vertex) + gravity
+        blocks = o.local_blocks(o.positions(x), 4 * st.contact.radius, st)[0].sum()
+        return blocks - float((sc.mesh.masses[:, None] * x * grav).sum())
+
+    eg, eo = potential(xg), potential(xo)
+    assert abs(eg - eo) <= RELATIVE_TOL * abs(eo), (eg, eo)
+
+
 # ---------------------------------------------------- reference known answers
 def test_resting_contact_settles_without_sawtooth_on_gpu():  # tests/vbd.rs:10-34
     for offset in ((0.0, 0.0, 0.0), (100.0, 101.4, -100.0)):

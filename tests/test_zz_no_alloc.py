@@ -58,16 +58,25 @@ def test_noalloc_radii_match_world_detect_on_two_calls_in_a_row():
     x_d = torch.from_numpy(x_all).to(dev)
     tri_d, edge_d, vf_d, ee_d = dev_u32(tris), dev_u32(edges), dev_u32(vf), dev_u32(ee)
     stream = torch.cuda.current_stream(dev)
-    outs = []
-    for _ in range(2):
-        radii_d = torch.full((moving,), -1.0, dtype=torch.float64, device=dev)
-        min_d = torch.full((1,), -1.0, dtype=torch.float64, device=dev)
+    # every output buffer exists before the calls, so the device's free memory
+    # can only change if the entry point itself allocates
+    bufs = [(torch.full((moving,), -1.0, dtype=torch.float64, device=dev),
+             torch.full((1,), -1.0, dtype=torch.float64, device=dev)) for _ in range(2)]
+    torch.cuda.synchronize()
+    outs, free = [], []
+    for radii_d, min_d in bufs:
+        free.append(torch.cuda.mem_get_info(dev)[0])
         rc = L.cc_ogc_radii_noalloc(
             x_d.data_ptr(), len(x_all), moving, tri_d.data_ptr(), len(tris), edge_d.data_ptr(), len(edges),
             vf_d.data_ptr(), len(vf), ee_d.data_ptr(), len(ee), rq, relaxation, radii_d.data_ptr(),
             min_d.data_ptr(), C.c_void_p(stream.cuda_stream))
         assert rc == abi.CC_OK
         torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info(dev)[0])
+    # the second call (its kernels already loaded by the first) leaves the
+    # device's free memory as it found it: no allocation on this path
+    assert free[3] == free[2], free
+    for radii_d, min_d in bufs:
         outs.append((radii_d.cpu().numpy(), float(min_d.item())))
     for radii, md in outs:
         assert np.array_equal(radii.view(np.uint64), ref["radii"].view(np.uint64))
