@@ -51,6 +51,7 @@ ITERATION_CAP = 200
 FIXED_ITERATIONS = 30
 STALL_REFRESH = 2  # refresh the OGC balls after 2 checks without a 5 % residual decrease
 ACCELERATION = 0.95  # Chebyshev spectral-radius estimate of the equal-residual legs
+SWEEP_PRECISION = 0  # sweep arithmetic of the timed legs: 0 FP64, 1 FP32 element assembly
 MLP_PATH = os.path.join(ROOT, "clothcraft_b200", "data", "fold_init_mlp.npz")
 UNIT = "steps/s"
 L2_FLUSH_BYTES = 256 << 20
@@ -190,11 +191,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def step_settings(sc, mode, iterations=None, acceleration=ACCELERATION):
+def step_settings(sc, mode, iterations=None, acceleration=ACCELERATION, precision=None):
     """Equal-residual settings (mode 0 adaptive, 1 learned) with the given
     Chebyshev acceleration, or a fixed iteration count with neither a
-    residual target nor acceleration when `iterations` is given."""
+    residual target nor acceleration when `iterations` is given. `precision`
+    is the sweep arithmetic (0 FP64, 1 FP32 assembly; default SWEEP_PRECISION)."""
     s = sc.settings
+    s.sweep_precision = SWEEP_PRECISION if precision is None else precision
     if iterations is None:
         s.iterations, s.residual_tolerance, s.residual_check_every = ITERATION_CAP, TOLERANCE, CHECK_EVERY
         s.stall_refresh = STALL_REFRESH
@@ -315,17 +318,19 @@ def main():
 
     # every solver after the first uses the lane variant the first one tuned,
     # so that all legs take the same trajectory bit for bit
-    tuned = {"lanes": args.lanes}
+    tuned = {"lanes": args.lanes, "lanes32": 0}
 
-    def make(mode, iterations=None, acceleration=ACCELERATION):
+    def make(mode, iterations=None, acceleration=ACCELERATION, precision=None):
         s = VbdSolver(sc)
         if tuned["lanes"] and L.cc_solver_set_lanes(s.h, tuned["lanes"]) != 0:
             raise SystemExit("invalid --lanes %d" % tuned["lanes"])
+        if tuned["lanes32"]:
+            s.set_lanes32(tuned["lanes32"])
         if mode:
             s.set_mlp(net, 1)
         s.set_state(*start)
         for _ in range(args.warmup):
-            s.step_resident(step_settings(sc, mode, iterations, acceleration))
+            s.step_resident(step_settings(sc, mode, iterations, acceleration, precision))
         return s
 
     def timed(solver, step_fn, k, host_clock=False):
@@ -375,6 +380,7 @@ def main():
     st_l, st_p = step_settings(sc, 1), step_settings(sc, 0)
     learned = make(1)
     tuned["lanes"] = int(L.cc_solver_get_lanes(learned.h))
+    tuned["lanes32"] = int(L.cc_solver_get_lanes32(learned.h))
     plain = make(0)
     warm_state = learned.get_state()
     clocks = ClockSampler(local).__enter__()
@@ -386,6 +392,15 @@ def main():
     L.cc_solver_set_profiling(learned.h, 0)
     # ---- plain adaptive init at equal residual
     t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
+    # ---- both inits at the other sweep precision (same target and acceleration)
+    other = 1 - SWEEP_PRECISION
+    other_legs = {}
+    for mode in (0, 1):
+        so = step_settings(sc, mode, precision=other)
+        solver_o = make(mode, precision=other)
+        if mode == 1 and other == 1:
+            tuned["lanes32"] = int(L.cc_solver_get_lanes32(solver_o.h))
+        other_legs[mode] = leg(solver_o, lambda: solver_o.step_resident(so), K)
     # ---- both inits without acceleration (the reference's iteration)
     unacc = {}
     for mode in (0, 1):
@@ -491,6 +506,11 @@ def main():
         "learned_vs_plain_time_ratio": t_p / t_l,
         "learned_init_used_fraction": float(np.mean([m["init_used"] for m in mets_l])),
         "acceleration": ACCELERATION,
+        "sweep_precision": ("fp32 element assembly" if SWEEP_PRECISION else "fp64"),
+        "other_precision": {"sweep_precision": ("fp32 element assembly" if other else "fp64"),
+                            "learned": summary(*other_legs[1]), "plain": summary(*other_legs[0]),
+                            "learned_vs_plain_time_ratio": other_legs[0][0] / other_legs[1][0],
+                            "lanes32": tuned["lanes32"]},
         "unaccelerated": {"learned": summary(*unacc[1]), "plain": summary(*unacc[0]),
                           "learned_vs_plain_time_ratio": unacc[0][0] / unacc[1][0],
                           "note": "same residual target, Chebyshev acceleration off (the reference's iteration)"},

@@ -84,7 +84,13 @@ class cc_vbd_settings(C.Structure):
         ("residual_check_every", C.c_uint32),
         ("stall_refresh", C.c_uint32),
         ("acceleration", C.c_double),
+        ("sweep_precision", C.c_uint32),
+        ("reserved1", C.c_uint32),
     ]
+
+
+CC_SWEEP_FP64 = 0
+CC_SWEEP_FP32 = 1
 
 
 class cc_grab(C.Structure):

@@ -20,6 +20,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 UNITS = {
     "detect.cu": ["--fmad=false"],
     "sweep.cu": [],
+    "sweep32.cu": [],
+    "radix.cu": [],
     "color.cu": [],
     "learned.cu": [],
     "mlp_tc.cu": [],

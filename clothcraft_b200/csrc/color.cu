@@ -10,7 +10,6 @@
 // longest descending chain, and contact edges between folded layers make
 // chains of length ~n; k_color_chunked below bounds the work by walking
 // index-ordered chunks instead.
-#include <cub/device/device_radix_sort.cuh>
 
 #include "color.cuh"
 
@@ -233,15 +232,7 @@ void Coloring::compute(const ColorView& view, cudaStream_t s) {
     // colour does not change any result (no two vertices of a colour interact).
     int bits = 1;
     while ((1u << bits) < n_colors_) ++bits;
-    size_t need = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, need, cur_, b_.ptr, iota_.ptr, order_.ptr, (int)n, 0, bits, s);
-    if (need > sort_tmp_bytes_) {
-        sort_tmp_.reserve(need);
-        sort_tmp_bytes_ = need;
-    }
-    CC_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp_.ptr, need, cur_, b_.ptr, iota_.ptr, order_.ptr, (int)n, 0, bits,
-                                            s));
-    launches_ += 2;
+    launches_ += sorter_.sort_pairs(cur_, b_.ptr, iota_.ptr, order_.ptr, n, bits, s);
     CC_CUDA(cudaGetLastError());
 }
 

@@ -34,8 +34,7 @@ class Coloring {
     DBuf<uint16_t> a_, b_;
     uint16_t* cur_ = nullptr;
     DBuf<uint32_t> order_, counts_, iota_;
-    DBuf<unsigned char> sort_tmp_;
-    size_t sort_tmp_bytes_ = 0;
+    RadixSorter sorter_;
     DBuf<unsigned int> changed_;
     Pinned<unsigned int> changed_h_;
     Pinned<uint32_t> counts_h_;

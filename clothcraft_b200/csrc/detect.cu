@@ -10,8 +10,6 @@
 // (on a miss) Morton LBVH build + dual-tree-equivalent pair queries ->
 // FP64 narrow phase -> radix sort + dedup of contact keys -> incidence CSR ->
 // per-vertex minimum distance -> conservative radii.
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -220,15 +218,7 @@ int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaSt
     k_bounds_init<<<1, 32, 0, s>>>(bounds.ptr);
     k_centroid_bounds<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr);
     k_morton<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr, morton_tmp.ptr, ids_tmp.ptr);
-    size_t need = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, need, morton_tmp.ptr, morton.ptr, ids_tmp.ptr, leaf_prim.ptr, (int)m,
-                                    0, 63, s);
-    if (need > sort_tmp_bytes) {
-        sort_tmp.reserve(need);
-        sort_tmp_bytes = need;
-    }
-    CC_CUDA(cub::DeviceRadixSort::SortPairs(sort_tmp.ptr, need, morton_tmp.ptr, morton.ptr, ids_tmp.ptr,
-                                            leaf_prim.ptr, (int)m, 0, 63, s));
+    int sorts = sorter.sort_pairs(morton_tmp.ptr, morton.ptr, ids_tmp.ptr, leaf_prim.ptr, m, 63, s);
     if (m > 1) {
         k_karras<<<grid_for(m - 1, 256), 256, 0, s>>>(morton.ptr, (int)m, child.ptr, parent.ptr);
         CC_CUDA(cudaMemsetAsync(visits.ptr, 0, (m - 1) * sizeof(unsigned), s));
@@ -236,7 +226,7 @@ int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaSt
                                                       visits.ptr, node_box.ptr, node_max.ptr);
     }
     CC_CUDA(cudaGetLastError());
-    return m > 1 ? 5 : 3;
+    return (m > 1 ? 5 : 3) + sorts;
 }
 
 // Stack traversal over the primitives with id > `above` only: subtrees whose
@@ -1185,27 +1175,17 @@ void World::detect(double query_radius, double radius, double relaxation, double
         raw_idx_s_.reserve(n_raw);
         uniq_flag_.reserve(n_raw);
         uniq_pos_.reserve(n_raw);
-        size_t need = 0, need2 = 0;
         const int lo_bits = (int)(2 * nb), hi_bits = (int)(2 * nb + 2);
-        cub::DeviceRadixSort::SortPairs(nullptr, need, raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_idx_s_.ptr,
-                                        (int)n_raw, 0, hi_bits, stream_);
-        cub::DeviceScan::ExclusiveSum(nullptr, need2, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw, stream_);
-        need = std::max(need, need2);
-        if (need > cub_tmp_bytes_) {
-            cub_tmp_.reserve(need);
-            cub_tmp_bytes_ = need;
-        }
-        CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.ptr, need, raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr,
-                                                raw_idx_s_.ptr, (int)n_raw, 0, lo_bits, stream_));
+        launches_ += sorter_.sort_pairs(raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_idx_s_.ptr, n_raw, lo_bits,
+                                        stream_);
         // gather hi in lo order, then stable sort by hi
         k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_idx_s_.ptr, raw_hi_s_.ptr, n_raw);
-        CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.ptr, need, raw_hi_s_.ptr, raw_hi_.ptr, raw_idx_s_.ptr,
-                                                raw_idx_.ptr, (int)n_raw, 0, hi_bits, stream_));
+        launches_ += sorter_.sort_pairs(raw_hi_s_.ptr, raw_hi_.ptr, raw_idx_s_.ptr, raw_idx_.ptr, n_raw, hi_bits,
+                                        stream_);
         // raw_hi_ = sorted hi, raw_idx_ = original index; gather lo
         k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_lo_.ptr, raw_idx_.ptr, raw_lo_s_.ptr, n_raw);
         k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, n_raw, uniq_flag_.ptr);
-        CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, uniq_flag_.ptr, uniq_pos_.ptr, (int)n_raw,
-                                              stream_));
+        launches_ += exclusive_sum(uniq_flag_.ptr, uniq_pos_.ptr, n_raw, scan_tmp_, stream_);
         k_unique_count<<<1, 1, 0, stream_>>>(uniq_flag_.ptr, uniq_pos_.ptr, n_raw, &sd->n_contacts);
         ++launches_;
         c_kind_.reserve(n_raw);
@@ -1225,16 +1205,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
                                                                       &sd->active);
         ++launches_;
     }
-    {
-        size_t need = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1), stream_);
-        if (need > cub_tmp_bytes_) {
-            cub_tmp_.reserve(need);
-            cub_tmp_bytes_ = need;
-        }
-        CC_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.ptr, need, inc_count_.ptr, inc_off_.ptr, (int)(moving_ + 1),
-                                              stream_));
-    }
+    launches_ += exclusive_sum(inc_count_.ptr, inc_off_.ptr, moving_ + 1, scan_tmp_, stream_);
     size_t n_inc_bound = 4 * n_raw;  // at most 4 moving vertices per contact
     inc_.reserve(std::max<size_t>(n_inc_bound, 1));
     if (n_raw > 0) {

@@ -5,9 +5,6 @@
 // warm start, colour sweeps with refresh detections, final feasibility and
 // trust-region checks, commit and history record. The host only sequences
 // kernels and reads a few scalars between phases.
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_reduce.cuh>
-#include <cub/device/device_scan.cuh>
 #include <chrono>
 #include <cmath>
 #include <memory>
@@ -53,7 +50,8 @@ bool vbd_valid(const cc_vbd_settings& s) {  // src/vbd.rs:38-51
     return ogc_valid(s.contact) && std::isfinite(s.dt) && s.dt >= 1e-6 && s.dt <= 0.025 && s.iterations != 0 &&
            s.iterations <= 200 && std::isfinite(s.damping) && s.damping >= 0.0 && std::isfinite(s.gravity[0]) &&
            std::isfinite(s.gravity[1]) && std::isfinite(s.gravity[2]) && std::isfinite(s.acceleration) &&
-           s.acceleration >= 0.0 && s.acceleration < 1.0;
+           s.acceleration >= 0.0 && s.acceleration < 1.0 &&
+           (s.sweep_precision == CC_SWEEP_FP64 || s.sweep_precision == CC_SWEEP_FP32) && s.reserved1 == 0;
 }
 }  // namespace
 
@@ -433,6 +431,7 @@ struct cc_solver {
     DBuf<double4> tri_coef;
     DBuf<double> tri_area;
     DBuf<MatParams> mats;
+    DBuf<MatParams32> mats32;
     DBuf<uint4> hinge_v;
     DBuf<double> hinge_k;
     DBuf<uint32_t> st_off, st_v;
@@ -456,14 +455,15 @@ struct cc_solver {
     // metrics scratch
     DBuf<unsigned long long> ext_key, ext_key_s, p95_bits;
     DBuf<double> ext_w, ext_w_s, ext_cum;
-    DBuf<unsigned char> cub_tmp;
-    size_t cub_bytes = 0;
+    RadixSorter ext_sorter;
+    DBuf<double> ext_scan;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tune0 = nullptr, tune1 = nullptr;
     bool profiling = false;
     std::vector<cudaEvent_t> prof_events;
     uint64_t own_launches = 0;
     uint32_t n_free = 0;
     int lanes = 0;          // vertices are solved by groups of `lanes` threads; 0 = autotune on next step
+    int lanes32 = 0;        // the same for the FP32-assembly sweep
     DBuf<double4> x_backup;
     std::vector<double> tune_ms;
     // objective and relative residual
@@ -522,6 +522,7 @@ struct cc_solver {
         v.tri_coef = tri_coef.ptr;
         v.tri_area = tri_area.ptr;
         v.mats = mats.ptr;
+        v.mats32 = mats32.ptr;
         v.hinge_v = hinge_v.ptr;
         v.hinge_k = hinge_k.ptr;
         v.st_off = st_off.ptr;
@@ -575,7 +576,11 @@ struct cc_solver {
     }
 
     void step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out);
-    void autotune(const SweepView& sv);
+    void autotune(const SweepView& sv, bool fp32);
+    void sweep(const SweepView& sv, const uint32_t* order, uint32_t count, bool fp32) {
+        if (fp32) launch_sweep32(sv, order, count, lanes32, stream);
+        else launch_sweep(sv, order, count, lanes, stream);
+    }
     ObjectiveCounts counts() const {
         return ObjectiveCounts{n_tri, n_hinge, n_stitch, world->stats().n_contacts};
     }
@@ -636,12 +641,17 @@ struct cc_solver {
 
 // Project autotuner: time one full colour sweep per candidate group width on
 // a backup of the positions (restored after each trial) and keep the fastest.
-void cc_solver::autotune(const SweepView& sv_in) {
+void cc_solver::autotune(const SweepView& sv_in, bool fp32) {
     // lanes per vertex | register cap (resident 128-thread blocks per SM: 3, 4, 5,
     // 6 or 8; above 3 the compiler spills to local memory) << 8
-    static const int kCandidates[] = {1 | 3 << 8,  2 | 3 << 8,  4 | 3 << 8,  4 | 4 << 8,  4 | 5 << 8,  4 | 6 << 8,
-                                      8 | 3 << 8,  8 | 4 << 8,  8 | 5 << 8,  8 | 6 << 8,  8 | 8 << 8,  16 | 3 << 8,
-                                      16 | 4 << 8, 16 | 6 << 8, 16 | 8 << 8, 32 | 3 << 8};
+    static const int kCandidates64[] = {1 | 3 << 8,  2 | 3 << 8,  4 | 3 << 8,  4 | 4 << 8,  4 | 5 << 8,  4 | 6 << 8,
+                                        8 | 3 << 8,  8 | 4 << 8,  8 | 5 << 8,  8 | 6 << 8,  8 | 8 << 8,  16 | 3 << 8,
+                                        16 | 4 << 8, 16 | 6 << 8, 16 | 8 << 8, 32 | 3 << 8};
+    static const int kCandidates32[] = {4 | 3 << 8,  4 | 4 << 8,  8 | 3 << 8,  8 | 4 << 8,  8 | 5 << 8,
+                                        8 | 6 << 8,  8 | 8 << 8,  16 | 3 << 8, 16 | 4 << 8, 16 | 6 << 8,
+                                        16 | 8 << 8, 32 | 3 << 8, 32 | 4 << 8};
+    const int* cands = fp32 ? kCandidates32 : kCandidates64;
+    const size_t n_cands = fp32 ? sizeof(kCandidates32) / sizeof(int) : sizeof(kCandidates64) / sizeof(int);
     SweepView sv = sv_in;  // trial sweeps never skip and count into a scratch counter
     sv.skip_at = nullptr;
     sv.clipped = &sc.ptr->clipped;
@@ -650,14 +660,17 @@ void cc_solver::autotune(const SweepView& sv_in) {
     const auto& off = coloring.offsets();
     tune_ms.clear();
     float best = 1e30f;
-    int best_g = 8 | 3 << 8;
-    for (int g : kCandidates) {
+    int best_g = fp32 ? (8 | 4 << 8) : (8 | 3 << 8);
+    for (size_t ci = 0; ci < n_cands; ++ci) {
+        const int g = cands[ci];
         float total = 1e30f;
         for (int rep = 0; rep < 4; ++rep) {  // first repetition warms caches; keep the fastest of the rest
             CC_CUDA(cudaEventRecord(tune0, stream));
             for (int sweep = 0; sweep < 2; ++sweep)  // two consecutive sweeps, as the iterations run
-                for (uint32_t c = 0; c < coloring.n_colors(); ++c)
-                    launch_sweep(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
+                for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
+                    if (fp32) launch_sweep32(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
+                    else launch_sweep(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
+                }
             CC_CUDA(cudaEventRecord(tune1, stream));
             CC_CUDA(cudaMemcpyAsync(world->x(), x_backup.ptr, n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
             CC_CUDA(cudaEventSynchronize(tune1));
@@ -674,7 +687,8 @@ void cc_solver::autotune(const SweepView& sv_in) {
         }
     }
     CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped, 0, sizeof(unsigned int), stream));
-    lanes = best_g;
+    if (fp32) lanes32 = best_g;
+    else lanes = best_g;
 }
 
 // MLP correction of the adaptive guess at three scales, clipped to the OGC
@@ -820,7 +834,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         }
         SweepView sv = sweep_view(cv, s, grab);
         sv.skip_at = &sc.ptr->stop_at;
-        if (lanes == 0) autotune(sv);
+        const bool fp32 = s.sweep_precision == CC_SWEEP_FP32;
+        if ((fp32 ? lanes32 : lanes) == 0) autotune(sv, fp32);
         // the Chebyshev sequence restarts with every batch (the step's start or a refresh)
         double4* acc_prev1 = acc_a.ptr;
         double4* acc_prev2 = acc_b.ptr;
@@ -856,7 +871,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                 for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
                     uint32_t cnt = off[c + 1] - off[c];
                     if (cnt == 0) continue;
-                    launch_sweep(sv, coloring.order() + off[c], cnt, lanes, stream);
+                    sweep(sv, coloring.order() + off[c], cnt, fp32);
                     ++own_launches;
                 }
                 if (profiling) {
@@ -960,18 +975,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         k_stretch<<<grid_for(n_tri, 256), 256, 0, stream>>>(n_tri, tri_v.ptr, tri_coef.ptr, tri_area.ptr, x0.ptr,
                                                             ext_key.ptr, ext_w.ptr);
         own_launches += 2;  // k_stretch and k_p95
-        size_t need = 0, need2 = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, need, ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr, (int)n_tri,
-                                        0, 64, stream);
-        cub::DeviceScan::InclusiveSum(nullptr, need2, ext_w_s.ptr, ext_cum.ptr, (int)n_tri, stream);
-        need = std::max(need, need2);
-        if (need > cub_bytes) {
-            cub_tmp.reserve(need);
-            cub_bytes = need;
-        }
-        CC_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp.ptr, need, ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr,
-                                                (int)n_tri, 0, 64, stream));
-        CC_CUDA(cub::DeviceScan::InclusiveSum(cub_tmp.ptr, need, ext_w_s.ptr, ext_cum.ptr, (int)n_tri, stream));
+        own_launches += ext_sorter.sort_pairs(ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr, n_tri, 64, stream);
+        own_launches += inclusive_sum(ext_w_s.ptr, ext_cum.ptr, n_tri, ext_scan, stream);
         double total = 0.0;
         unsigned long long kmax = 0, kp = order_key(0.0);
         CC_CUDA(cudaMemcpyAsync(&total, ext_cum.ptr + n_tri - 1, 8, cudaMemcpyDeviceToHost, stream));
@@ -1239,6 +1244,12 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
             if (!(mesh->masses[i] > 0.0) || !std::isfinite(mesh->masses[i]))
                 throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid material binding or mesh topology"};
         h->mats.upload(mats, st);
+        {
+            std::vector<MatParams32> m32;
+            for (const MatParams& M : mats)
+                m32.push_back({(float)M.warp, (float)M.weft, (float)M.shear, (float)M.c, (float)M.delta});
+            h->mats32.upload(m32, st);
+        }
         h->tri_v.upload(tv, st);
         h->tri_coef.upload(tc, st);
         h->tri_area.upload(ta, st);
@@ -1320,6 +1331,17 @@ int32_t cc_solver_set_lanes(cc_solver* s, int32_t lanes) {
     return CC_OK;
 }
 int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes; }
+int32_t cc_solver_set_lanes32(cc_solver* s, int32_t lanes) {
+    int32_t g = lanes & 0xff, cap = lanes >> 8;
+    if (!(g == 0 || g == 4 || g == 8 || g == 16 || g == 32) ||
+        !(cap == 0 || cap == 3 || cap == 4 || cap == 5 || cap == 6 || cap == 8) || (g == 0 && cap != 0))
+        return s->fail(Failure{CC_ERR_INVALID_ARGUMENT,
+                               "FP32 sweep lanes must be 0 (autotune), 4, 8, 16 or 32, optionally | cap << 8 "
+                               "with cap 3, 4, 5, 6 or 8"});
+    s->lanes32 = lanes == 0 ? 0 : (g | (cap ? cap : 3) << 8);
+    return CC_OK;
+}
+int32_t cc_solver_get_lanes32(const cc_solver* s) { return s->lanes32; }
 cc_world* cc_solver_world(cc_solver* s) { return &s->world_view; }
 
 static void upload_state(cc_solver* s, const double* x, const double* v) {

@@ -7,6 +7,9 @@ namespace cc {
 struct MatParams {  // per material, membrane part (src/energy.rs:10-29)
     double warp, weft, shear, c, delta;
 };
+struct MatParams32 {  // the same, rounded to FP32 for the FP32-assembly sweep
+    float warp, weft, shear, c, delta;
+};
 
 // Packed incidence entry: type (2 bits) | slot (2 bits) | index (28 bits).
 enum TermType : uint32_t { TERM_TRI = 0, TERM_HINGE = 1, TERM_STITCH = 2 };
@@ -35,6 +38,7 @@ struct SweepView {
     const double4* tri_coef;    // w = ds0*c.x + ds1*c.y ; v = ds0*c.z + ds1*c.w (grain-rotated inv_dm)
     const double* tri_area;
     const MatParams* mats;
+    const MatParams32* mats32;
     const uint4* hinge_v;
     const double* hinge_k;      // 0.5 * weight * (bend_warp aw^2 + bend_weft af^2)
     const uint32_t* st_off;
@@ -62,6 +66,8 @@ constexpr int kSumBlocks = 296;  // 2 x 148 SMs
 
 // launch helpers (sweep.cu)
 void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
+// FP32 element assembly (sweep32.cu); lanes 4, 8, 16 or 32 | cap << 8
+void launch_sweep32(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
 void launch_local_blocks(const SweepView& s, double* energy, double* grad, double* hess, cudaStream_t st);
 // out[v] = |dE/dx_v|^2 over moving vertices (variant as launch_sweep); with
 // `project`, the KKT residual of the OGC-ball constraints (sweep.cu)

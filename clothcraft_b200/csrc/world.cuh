@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "radix.cuh"
 
 namespace cc {
 
@@ -33,8 +34,7 @@ struct Lbvh {
     DBuf<uint32_t> leaf_prim, ids_tmp;
     DBuf<unsigned long long> morton, morton_tmp;
     DBuf<unsigned long long> bounds;  // 6 order keys
-    DBuf<unsigned char> sort_tmp;
-    size_t sort_tmp_bytes = 0;
+    RadixSorter sorter;
     // returns the number of this library's kernels launched
     int build(const Box* prim_box, const uint32_t* ids, uint32_t m, cudaStream_t s);
     LbvhView view(const Box* prim_box) const {
@@ -165,8 +165,8 @@ class World {
     DBuf<double> radii_;
     DBuf<double4> centers_;
     DBuf<uint32_t> inc_count_, inc_off_, inc_, inc_cursor_;
-    DBuf<unsigned char> cub_tmp_;
-    size_t cub_tmp_bytes_ = 0;
+    RadixSorter sorter_;
+    DBuf<uint32_t> scan_tmp_;
     DBuf<DetectStats> stats_d_;
     Pinned<DetectStats> stats_h_;
     double query_radius_ = 0;

@@ -38,6 +38,8 @@ SIGNATURES = {
     "cc_solver_set_profiling": (C.c_int32, [C.c_void_p, C.c_int32]),
     "cc_solver_set_lanes": (C.c_int32, [C.c_void_p, C.c_int32]),
     "cc_solver_get_lanes": (C.c_int32, [C.c_void_p]),
+    "cc_solver_set_lanes32": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "cc_solver_get_lanes32": (C.c_int32, [C.c_void_p]),
     "cc_solver_colors": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_ogc_settings),
                                      C.POINTER(cc_grab), c_uint32_p, c_uint32_p]),
     "cc_solver_local_blocks": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_vbd_settings),

@@ -31,11 +31,15 @@ def main(argv=None):
     ap.add_argument("--learned", action="store_true")
     ap.add_argument("--fixed", type=int, default=0)
     ap.add_argument("--acceleration", type=float, default=0.0)
+    ap.add_argument("--precision", type=int, default=0, help="sweep arithmetic: 0 FP64, 1 FP32 assembly")
+    ap.add_argument("--lanes32", type=int, default=8 | 4 << 8)
+    ap.add_argument("--profile", action="store_true", help="time each iteration's sweeps with CUDA events")
     args = ap.parse_args(argv)
     sc = scenes.config1()
     z = np.load(FOLD_STATE)
-    g = VbdSolver(sc).set_lanes(args.lanes)
+    g = VbdSolver(sc).set_lanes(args.lanes).set_lanes32(args.lanes32)
     s = sc.settings
+    s.sweep_precision = args.precision
     if args.fixed:
         s.iterations = args.fixed
     else:
@@ -47,10 +51,12 @@ def main(argv=None):
         g.set_mlp(Mlp.load(os.path.join(HERE, "data", "fold_init_mlp.npz")), 1)
         s.init_mode = 1
     g.set_state(z["x"].astype(np.float64), z["v"].astype(np.float64), float(z["time"]))
+    g.set_profiling(args.profile)
     for k in range(args.steps):
         m = g.step_resident(s.to_c())
-        print("step %d: %d iterations, %.2f ms, residual %s" % (k, m["iterations"], m["gpu_compute_ms"],
-                                                              m["relative_residual"]), flush=True)
+        print("step %d: %d iterations, %.2f ms, residual %s, sweeps %.3f ms in %d launches" % (
+            k, m["iterations"], m["gpu_compute_ms"], m["relative_residual"], m["sweep_ms"], m["sweep_launches"]),
+            flush=True)
 
 
 if __name__ == "__main__":

@@ -357,6 +357,7 @@ class StepSettings:
     residual_check_every: int = 0
     stall_refresh: int = 0
     acceleration: float = 0.0  # Chebyshev rho; 0 = off (the reference)
+    sweep_precision: int = 0  # 0 FP64 sweeps (the CPU path's arithmetic), 1 FP32 element assembly
 
     def to_c(self) -> abi.cc_vbd_settings:
         s = abi.cc_vbd_settings()
@@ -367,6 +368,7 @@ class StepSettings:
         s.residual_check_every = self.residual_check_every
         s.stall_refresh = self.stall_refresh
         s.acceleration = self.acceleration
+        s.sweep_precision = self.sweep_precision
         s.damping = self.damping
         for k in range(3):
             s.gravity[k] = self.gravity[k]

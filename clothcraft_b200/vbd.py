@@ -285,6 +285,20 @@ class VbdSolver:
             raise self._err(rc)
         return self
 
+    def set_profiling(self, enable: bool):
+        """Time each iteration's colour sweeps with CUDA events (metrics
+        sweep_ms); the kernels themselves are unchanged."""
+        native.load().cc_solver_set_profiling(self.h, 1 if enable else 0)
+        return self
+
+    def set_lanes32(self, lanes: int):
+        """Threads per vertex solve of the FP32-assembly sweep (4, 8, 16 or 32,
+        optionally | cap << 8), or 0 to autotune on the next FP32 step."""
+        rc = native.load().cc_solver_set_lanes32(self.h, int(lanes))
+        if rc != 0:
+            raise self._err(rc)
+        return self
+
     def last_step_trace(self):
         """(relative residual after each iteration, NaN where not evaluated;
         vertices clipped in each iteration) of the last step."""

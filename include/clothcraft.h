@@ -101,6 +101,19 @@ enum cc_init_mode {
     CC_INIT_LEARNED = 1   /* MLP correction of the adaptive guess, kept only */
                           /* when its step energy is lower (cc_mlp_*)        */
 };
+/* Arithmetic of the colour sweeps (no reference counterpart; the reference's
+ * CPU path is FP64, its wgpu shader FP32).
+ * CC_SWEEP_FP64: every term and the 3x3 solve in FP64, operation for operation
+ *   as the CPU path (the parity form).
+ * CC_SWEEP_FP32: membrane and bending energies, gradients and Hessians in FP32
+ *   from FP64 edge differences; OGC contact terms in FP64; the 3x3 solve in
+ *   FP32 unless its condition estimate exceeds 1e6; the line search compares
+ *   energy differences summed in FP64. Detection, the relative residual and
+ *   the step energy stay FP64. */
+enum cc_sweep_precision {
+    CC_SWEEP_FP64 = 0,
+    CC_SWEEP_FP32 = 1
+};
 /* VbdSettings (src/vbd.rs:18-52), plus two extensions without a reference
  * counterpart: the initial-guess mode and a relative-residual target.
  *
@@ -140,6 +153,8 @@ typedef struct cc_vbd_settings {
     uint32_t residual_check_every;   /* 0 = no relative residual            */
     uint32_t stall_refresh;          /* 0 = off                             */
     double acceleration;             /* Chebyshev rho in [0, 1); 0 = off     */
+    uint32_t sweep_precision;        /* cc_sweep_precision                  */
+    uint32_t reserved1;              /* must be 0                           */
 } cc_vbd_settings;
 
 /* Grab (src/vbd.rs:54-60): mouse attachment, weights sum to one. */
@@ -288,6 +303,11 @@ int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
  * workgroup per vertex, src/vbd.wgsl:118-150). */
 int32_t cc_solver_set_lanes(cc_solver* solver, int32_t lanes);
 int32_t cc_solver_get_lanes(const cc_solver* solver);
+/* The same for the CC_SWEEP_FP32 sweep: lanes 4, 8, 16 or 32, optionally
+ * | (cap << 8) with cap = 3, 4, 5, 6 or 8; 0 (the default) autotunes on the
+ * first FP32 step. */
+int32_t cc_solver_set_lanes32(cc_solver* solver, int32_t lanes);
+int32_t cc_solver_get_lanes32(const cc_solver* solver);
 
 /* The solver's OGC world (owned by the solver; do not destroy). */
 cc_world* cc_solver_world(cc_solver* solver);

@@ -41,6 +41,6 @@ def test_abi_version_and_no_device_is_reported_not_faked():
 def test_struct_layouts_match_header_sizes():
     # field order/size mirrors include/clothcraft.h (LP64)
     assert C.sizeof(abi.cc_material) == 80
-    assert C.sizeof(abi.cc_vbd_settings) == 8 + 8 + 8 + 24 + 32 + 16 + 8
+    assert C.sizeof(abi.cc_vbd_settings) == 8 + 8 + 8 + 24 + 32 + 16 + 8 + 8
     assert C.sizeof(abi.cc_grab) == 16 + 24 + 24 + 8
     assert C.sizeof(abi.cc_mesh) == 21 * 8
