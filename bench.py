@@ -465,11 +465,16 @@ def main():
     det_ms = sum(m["detection_ms"] for m in mets_l) / K
     col_ms = sum(m["color_ms"] for m in mets_l) / K
     init_ms = sum(m["init_ms"] for m in mets_l) / K
-    breakdown = {"detection": det_ms, "coloring": col_ms, "learned_guess": init_ms, "sweeps": sweep_ms / K,
+    det_dev = {k: sum(m[k + "_ms"] for m in mets_l) / K for k in ("refit", "candidates", "narrow")}
+    breakdown = {"detection": det_ms, "detection_device": det_dev, "coloring": col_ms, "learned_guess": init_ms,
+                 "sweeps": sweep_ms / K,
                  "other": t_l / K - det_ms - col_ms - init_ms - sweep_ms / K,
                  "note": "from the timed learned leg: detection and colouring by host clock (they end in a "
-                         "device sync), learned guess and sweeps by CUDA events; other = ms_per_step minus "
-                         "the four (predict, warm start, residual checks, acceleration, commit, metrics)"}
+                         "device sync), learned guess and sweeps by CUDA events; detection_device = the "
+                         "detection phases by CUDA events (refit and cache check, candidate rebuilds, narrow "
+                         "phase with the canonical sort, incidence and radii); other = ms_per_step minus "
+                         "detection, colouring, learned guess and sweeps (predict, warm start, residual "
+                         "checks, acceleration, commit, metrics)"}
 
     # ---- CPU baseline (rank 0, N=1 only): the oracle at equal residual from
     # the state the timed legs start from, a sample of about 30 s

@@ -998,7 +998,10 @@ World::World(const double* x_all, size_t n_all, const std::vector<std::array<uin
     CC_CUDA(cudaStreamSynchronize(stream_));
 }
 
-World::~World() {}
+World::~World() {
+    for (cudaEvent_t e : phase_ev_)
+        if (e) cudaEventDestroy(e);
+}
 
 WorldView World::view() const {
     return {(uint32_t)n_all_,
@@ -1101,11 +1104,18 @@ __global__ void k_reset_stats(DetectStats* s, double query_radius) {
     s->rebuild = 0;
 }
 
+void World::mark(int k) {
+    if (!profile_) return;
+    if (!phase_ev_[k]) CC_CUDA(cudaEventCreate(&phase_ev_[k]));
+    CC_CUDA(cudaEventRecord(phase_ev_[k], stream_));
+}
+
 void World::detect(double query_radius, double radius, double relaxation, double stiffness, bool check_fixed,
                    bool prune) {
     (void)stiffness;
     query_radius_ = query_radius;
     DetectStats* sd = stats_d_.ptr;
+    mark(0);
     // reset per-detection counters (keep n_vf/n_ee of the cache)
     k_reset_stats<<<1, 1, 0, stream_>>>(sd, query_radius);
     refit(check_fixed);
@@ -1113,6 +1123,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
                                                                    &sd->max_move_bits, &sd->max_abs_bits);
     launches_ += 2;
     CC_CUDA(cudaGetLastError());
+    mark(1);
     sync_stats();
     raise_device_error(stats_h_.ptr->error);
     double max_move;
@@ -1131,6 +1142,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
         CC_CUDA(cudaMemcpyAsync(cache_centers_.ptr, x_.ptr, moving_ * sizeof(double4), cudaMemcpyDeviceToDevice,
                                 stream_));
     }
+    mark(2);
     unsigned long long n_vf = stats_h_.ptr->n_vf, n_ee = stats_h_.ptr->n_ee;
     // bits per vertex id in the contact keys: the radix sorts below run only
     // over the 2nb + 2 (hi) and 2nb (lo) bits the keys use
@@ -1155,6 +1167,7 @@ void World::detect(double query_radius, double radius, double relaxation, double
                                                                     &sd->max_abs_bits, prune ? 1 : 0, o);
         launches_ += 2;
         CC_CUDA(cudaGetLastError());
+        mark(3);
         sync_stats();
         if (stats_h_.ptr->n_raw <= raw_cap_) break;
         raw_cap_ = (size_t)(stats_h_.ptr->n_raw * 1.5) + 4096;
@@ -1222,9 +1235,18 @@ void World::detect(double query_radius, double radius, double relaxation, double
     CC_CUDA(cudaMemcpyAsync(&sd->n_incident, inc_off_.ptr + moving_, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                             stream_));
     CC_CUDA(cudaGetLastError());
+    mark(4);
     sync_stats();
     stats_h_.ptr->n_incident &= 0xffffffffull;
     stats_h_.ptr->rebuild = rebuild ? 1 : 0;
+    if (profile_) {
+        float t[4];
+        for (int k = 0; k < 4; ++k) CC_CUDA(cudaEventElapsedTime(&t[k], phase_ev_[k], phase_ev_[k + 1]));
+        phase_ms_.refit = t[0];
+        phase_ms_.candidates = t[1];
+        phase_ms_.narrow = t[2];
+        phase_ms_.canonical = t[3];
+    }
     raise_device_error(stats_h_.ptr->error);
 }
 

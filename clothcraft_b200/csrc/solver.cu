@@ -565,8 +565,15 @@ struct cc_solver {
 
     void detect(double rq, const cc_ogc_settings& s, cc_metrics* m, double& det_ms) {
         double t = now_ms();
+        world->set_profiling(profiling);
         world->detect(rq, s.radius, s.relaxation, s.stiffness, false);
         det_ms += now_ms() - t;
+        if (m && profiling) {
+            const World::PhaseMs& p = world->last_phase_ms();
+            m->refit_ms += p.refit;
+            m->candidates_ms += p.candidates;
+            m->narrow_ms += p.narrow + p.canonical;
+        }
         if (m) {
             m->detection_updates += 1;
             m->broad_phase_rebuilds += world->stats().rebuild;

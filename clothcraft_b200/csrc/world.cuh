@@ -124,6 +124,14 @@ class World {
     cudaStream_t stream() const { return stream_; }
     void invalidate_cache() { cache_valid_ = false; }
     uint64_t launches() const { return launches_; }
+    // Device time of the last detection's phases (CUDA events; recorded only
+    // while profiling is on): refit and cache check, candidate rebuild (0 on a
+    // cache hit), narrow phase, canonical set (sort, dedup, incidence, radii).
+    struct PhaseMs {
+        double refit = 0, candidates = 0, narrow = 0, canonical = 0;
+    };
+    void set_profiling(bool on) { profile_ = on; }
+    const PhaseMs& last_phase_ms() const { return phase_ms_; }
 
    private:
     WorldView view() const;
@@ -171,6 +179,10 @@ class World {
     Pinned<DetectStats> stats_h_;
     double query_radius_ = 0;
     uint64_t launches_ = 0;
+    bool profile_ = false;
+    cudaEvent_t phase_ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    PhaseMs phase_ms_;
+    void mark(int k);
 
     friend struct WorldAccess;
 };

@@ -54,9 +54,11 @@ def main(argv=None):
     g.set_profiling(args.profile)
     for k in range(args.steps):
         m = g.step_resident(s.to_c())
-        print("step %d: %d iterations, %.2f ms, residual %s, sweeps %.3f ms in %d launches" % (
-            k, m["iterations"], m["gpu_compute_ms"], m["relative_residual"], m["sweep_ms"], m["sweep_launches"]),
-            flush=True)
+        print("step %d: %d iterations, %.2f ms, residual %s, sweeps %.3f ms in %d launches, detection %.3f ms "
+              "host (%d; device refit %.3f candidates %.3f narrow %.3f), colouring %.3f ms" % (
+                  k, m["iterations"], m["gpu_compute_ms"], m["relative_residual"], m["sweep_ms"],
+                  m["sweep_launches"], m["detection_ms"], m["detection_updates"], m["refit_ms"],
+                  m["candidates_ms"], m["narrow_ms"], m["color_ms"]), flush=True)
 
 
 if __name__ == "__main__":

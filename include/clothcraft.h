@@ -170,7 +170,9 @@ typedef struct cc_grab {
 typedef struct cc_metrics {
     double time_s, dt_s, step_ms, detection_ms, solve_ms;
     double gpu_compute_ms;          /* device time of the step, CUDA events   */
-    double refit_ms, candidates_ms, narrow_ms;
+    double refit_ms, candidates_ms, narrow_ms; /* device time of the detection
+                                      phases (profiling on; narrow includes the
+                                      canonical sort, incidence and radii)    */
     uint64_t candidate_pairs, aabb_rejections;
     uint64_t iterations, contacts, contact_terms;
     uint64_t detection_updates, broad_phase_rebuilds, truncated_vertices;
