@@ -129,6 +129,23 @@ class cc_metrics(C.Structure):
         return d
 
 
+class cc_newton_report(C.Structure):
+    _fields_ = [
+        ("converged", C.c_int32),
+        ("iterations", C.c_uint32),
+        ("pcg_iterations", C.c_uint64),
+        ("residual_rms_n", C.c_double),
+        ("objective_j", C.c_double),
+        ("relative_force_residual", C.c_double),
+        ("contact_terms", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["converged"] = bool(d["converged"])
+        return d
+
+
 class cc_contacts(C.Structure):
     _fields_ = [
         ("contact_capacity", C.c_uint64),

@@ -22,6 +22,7 @@ UNITS = {
     "sweep.cu": [],
     "sweep32.cu": [],
     "radix.cu": [],
+    "newton.cu": [],
     "color.cu": [],
     "learned.cu": [],
     "mlp_tc.cu": [],

@@ -14,6 +14,7 @@
 #include "color.cuh"
 #include "learned.cuh"
 #include "sweep.cuh"
+#include "newton.cuh"
 #include "world.cuh"
 
 using namespace cc;
@@ -485,6 +486,9 @@ struct cc_solver {
     float* sample_targets = nullptr;
     cudaEvent_t learn0 = nullptr, learn1 = nullptr;
     bool learn_timed = false;
+    // Newton reference step (cc_solver_newton_step)
+    DBuf<double4> nt_x0, nt_v0, nt_guess, nt_target, nt_y, nt_out;
+    DBuf<double> nt_inertia;
     // batched instances (cc_batch_create): first vertex and count of each
     std::vector<uint64_t> inst_first, inst_count;
     std::string err;
@@ -1399,6 +1403,75 @@ int32_t cc_solver_step_resident(cc_solver* s, const cc_vbd_settings* settings, c
         return CC_OK;
     } catch (const Failure& f) {
         s->time = t0;
+        return s->fail(f);
+    }
+}
+
+int32_t cc_solver_newton_step(cc_solver* s, const double* x_old, const double* v_old,
+                              const cc_vbd_settings* settings, uint32_t newton_iterations, uint32_t pcg_iterations,
+                              double abs_tol, double rel_tol, double* x_out, cc_newton_report* report) {
+    try {
+        if (!settings || !vbd_valid(*settings) || !x_old || !v_old || !x_out || newton_iterations > 1000 ||
+            pcg_iterations == 0 || !(abs_tol >= 0.0) || !(rel_tol >= 0.0))
+            throw Failure{CC_ERR_INVALID_ARGUMENT, "Invalid Newton settings"};
+        const cc_vbd_settings& st = *settings;
+        const uint32_t n = s->n, n_all = s->n_all;
+        cudaStream_t stream = s->stream;
+        for (DBuf<double4>* b : {&s->nt_x0, &s->nt_v0, &s->nt_guess, &s->nt_target}) b->reserve(n);
+        s->nt_y.reserve(n_all);
+        s->nt_out.reserve(n_all);
+        s->nt_inertia.reserve(n);
+        // the caller's state in the device layout (the solver's own state is untouched)
+        s->io.reserve(6 * (size_t)n);
+        CC_CUDA(cudaMemcpyAsync(s->io.ptr, x_old, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        CC_CUDA(cudaMemcpyAsync(s->io.ptr + 3 * (size_t)n, v_old, 3 * (size_t)n * sizeof(double),
+                                cudaMemcpyHostToDevice, stream));
+        launch_unpack_state(n, s->io.ptr, s->nt_x0.ptr, s->nt_v0.ptr, stream);
+        // inertial target, inertia and the step's query radius (src/vbd.rs:283-307)
+        CC_CUDA(cudaMemsetAsync(s->sc.ptr, 0, sizeof(StepScalars), stream));
+        int gb = grid_for(n, 256);
+        double3 g3 = make_double3(st.gravity[0], st.gravity[1], st.gravity[2]);
+        k_predict<<<gb, 256, 0, stream>>>(n, s->nt_x0.ptr, s->nt_v0.ptr, s->accel.ptr, 0, s->sc.ptr, st.dt, g3,
+                                          st.damping, s->masses.ptr, s->nt_guess.ptr, s->nt_target.ptr,
+                                          s->nt_inertia.ptr, s->sc.ptr);
+        CC_CUDA(cudaGetLastError());
+        s->read_scalars();
+        double motion;
+        std::memcpy(&motion, &s->sc_h.ptr->motion_bits, 8);
+        double r = st.contact.radius;
+        double rq = std::min(std::max(r + motion, 2.0 * r), 4.0 * r);
+        // the step's OGC contact set at x_old, frozen for the whole solve
+        k_copy_positions<<<gb, 256, 0, stream>>>(n, s->nt_x0.ptr, s->world->x());
+        s->world->detect(rq, r, st.contact.relaxation, st.contact.stiffness, false);
+        ContactsView cv = s->world->contacts();
+        NewtonProblem pb;
+        pb.view = s->sweep_view(cv, st, nullptr);
+        pb.view.target = s->nt_target.ptr;
+        pb.view.inertia = s->nt_inertia.ptr;
+        pb.n_all = n_all;
+        pb.n_free = s->n_free;
+        pb.n_tri = s->n_tri;
+        pb.counts = s->counts();
+        CC_CUDA(cudaMemcpyAsync(s->nt_y.ptr, s->world->x(), n_all * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
+        k_copy_positions<<<gb, 256, 0, stream>>>(n, s->nt_target.ptr, s->nt_y.ptr);
+        pb.y_all = s->nt_y.ptr;
+        double gy2 = 0.0;
+        NewtonResult res = newton_solve(pb, s->world->x(), newton_iterations, pcg_iterations, abs_tol, rel_tol,
+                                        s->nt_out.ptr, &gy2, stream);
+        launch_pack_state(n, s->nt_out.ptr, s->nt_v0.ptr, s->io.ptr, stream);
+        CC_CUDA(cudaMemcpyAsync(x_out, s->io.ptr, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaStreamSynchronize(stream));
+        if (report) {
+            report->converged = res.converged ? 1 : 0;
+            report->iterations = res.iterations;
+            report->pcg_iterations = res.pcg_iterations;
+            report->residual_rms_n = res.residual_rms;
+            report->objective_j = res.objective;
+            report->relative_force_residual = gy2 > 0.0 ? std::sqrt(res.gradient_sq / gy2) : 0.0;
+            report->contact_terms = s->world->stats().n_contacts;
+        }
+        return CC_OK;
+    } catch (const Failure& f) {
         return s->fail(f);
     }
 }

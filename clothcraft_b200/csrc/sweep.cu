@@ -23,82 +23,6 @@
 
 namespace cc {
 
-// Partial sum of the incident terms dealt to `lane` of a group of G
-// (VbdSolver::local, src/vbd.rs:196-248).
-template <bool D, int G, bool HS = D>
-__device__ __forceinline__ double local_part(const SweepView& s, uint32_t v, d3 p, uint32_t lane, d3& g, Sym& H) {
-    double e = 0.0;
-    // entries are grouped by type: one lane-strided loop per type, no per-entry dispatch
-    uint32_t b0 = s.inc_off[v], b1 = s.inc_off[v + 1];
-    uint2 mid = s.inc_mid[v];
-    // each loop loads the next term's record before it evaluates the current one
-    {
-        uint32_t k = b0 + lane;
-        uint32_t ent = k < mid.x ? s.inc[k] : 0u;
-        int4 tv = make_int4(0, 0, 0, 0);
-        double4 cf = make_double4(0, 0, 0, 0);
-        double A = 0.0;
-        if (k < mid.x) {
-            uint32_t t = ent & 0x0fffffffu;
-            tv = s.tri_v[t];
-            cf = s.tri_coef[t];
-            A = s.tri_area[t];
-        }
-        for (; k < mid.x; k += G) {
-            uint32_t kn = k + G;
-            uint32_t en = 0u;
-            int4 tvn = tv;
-            double4 cfn = cf;
-            double An = A;
-            if (kn < mid.x) {
-                en = s.inc[kn];
-                uint32_t t = en & 0x0fffffffu;
-                tvn = s.tri_v[t];
-                cfn = s.tri_coef[t];
-                An = s.tri_area[t];
-            }
-            e += membrane_rec<D, HS>(s, tv, cf, A, (ent >> 28) & 3u, p, g, H);
-            ent = en;
-            tv = tvn;
-            cf = cfn;
-            A = An;
-        }
-    }
-    {
-        uint32_t k = mid.x + lane;
-        uint32_t ent = k < mid.y ? s.inc[k] : 0u;
-        uint4 hv = make_uint4(0, 0, 0, 0);
-        double K = 0.0;
-        if (k < mid.y) {
-            uint32_t h = ent & 0x0fffffffu;
-            hv = s.hinge_v[h];
-            K = s.hinge_k[h];
-        }
-        for (; k < mid.y; k += G) {
-            uint32_t kn = k + G;
-            uint32_t en = 0u;
-            uint4 hvn = hv;
-            double Kn = K;
-            if (kn < mid.y) {
-                en = s.inc[kn];
-                uint32_t h = en & 0x0fffffffu;
-                hvn = s.hinge_v[h];
-                Kn = s.hinge_k[h];
-            }
-            e += bending_rec<D, HS>(s, hv, K, (ent >> 28) & 3u, p, g, H);
-            ent = en;
-            hv = hvn;
-            K = Kn;
-        }
-    }
-    for (uint32_t k = mid.y + lane; k < b1; k += G) e += stitch_term<D>(s, s.inc[k] & 0x0fffffffu, v, p, g, H);
-    uint32_t c1 = s.contacts.inc_off[v + 1];
-    for (uint32_t k = s.contacts.inc_off[v] + lane; k < c1; k += G) e += contact_term<D>(s, s.contacts.inc[k], v, p, g, H);
-    if (lane == 0 && s.grab.active && (s.grab.v[0] == v || s.grab.v[1] == v || s.grab.v[2] == v))
-        e += grab_term<D>(s, v, p, g, H);
-    return e;
-}
-
 template <int G>
 __device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uint32_t lane, unsigned mask) {
     if (s.pinned[v]) {

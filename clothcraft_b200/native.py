@@ -10,7 +10,7 @@ import os
 from pathlib import Path
 
 from .abi import (c_double_p, c_uint32_p, cc_candidates, cc_contacts, cc_grab, cc_mesh, cc_metrics,
-                  cc_ogc_settings, cc_surface, cc_vbd_settings)
+                  cc_newton_report, cc_ogc_settings, cc_surface, cc_vbd_settings)
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libclothcraft_b200.so"
 _LIB = None
@@ -45,6 +45,9 @@ SIGNATURES = {
     "cc_solver_local_blocks": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_vbd_settings),
                                            C.POINTER(cc_grab), c_double_p, c_double_p, c_double_p, c_double_p,
                                            c_double_p]),
+    "cc_solver_newton_step": (C.c_int32, [C.c_void_p, c_double_p, c_double_p, C.POINTER(cc_vbd_settings),
+                                          C.c_uint32, C.c_uint32, C.c_double, C.c_double, c_double_p,
+                                          C.POINTER(cc_newton_report)]),
     "cc_world_create": (C.c_int32, [c_double_p, C.c_uint64, c_uint32_p, C.c_uint64, C.c_uint64, c_uint32_p,
                                     C.c_uint64, C.POINTER(C.c_void_p)]),
     "cc_world_destroy": (None, [C.c_void_p]),

@@ -339,6 +339,23 @@ class VbdSolver:
             raise self._err(rc)
         return m.as_dict()
 
+    def newton_step(self, x_old, v_old, settings, newton_iterations=30, pcg_iterations=500, abs_tol=1e-6,
+                    rel_tol=1e-4):
+        """FP64 Newton reference step on the GPU from (x_old, v_old) with the
+        step's OGC contacts frozen (src/solver.rs:422-646 plus the contact
+        terms). Returns (x, report dict); the solver's state is not changed."""
+        x_old = abi.as_f64(x_old)
+        v_old = abi.as_f64(v_old)
+        out = np.zeros((self.n, 3))
+        rep = abi.cc_newton_report()
+        s = _settings_c(settings)
+        rc = native.load().cc_solver_newton_step(self.h, _f64p(x_old), _f64p(v_old), C.byref(s),
+                                                 int(newton_iterations), int(pcg_iterations), float(abs_tol),
+                                                 float(rel_tol), _f64p(out), C.byref(rep))
+        if rc != 0:
+            raise self._err(rc)
+        return out, rep.as_dict()
+
     def colors(self, x_all, query_radius, ogc, grab=None):
         x_all = abi.as_f64(x_all)
         out = np.zeros(self.n, np.uint32)

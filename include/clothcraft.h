@@ -332,6 +332,30 @@ int32_t cc_solver_local_blocks(cc_solver* solver, const double* x_all,
                                const double* inertia, double* energy,
                                double* gradient, double* hessian);
 
+/* FP64 Newton reference step on the GPU, for residual and error references at
+ * scale (ReferenceSolver::step_problem, src/solver.rs:422-646: Newton on the
+ * implicit-Euler objective, Jacobi-preconditioned CG with shift escalation,
+ * Armijo backtracking, stop at RMS gradient <= max(abs_tol, rel_tol r0)).
+ * The reference's Newton solver has no OGC term; here the step's contact set,
+ * detected at x_old with the step's query radius, enters frozen with
+ * Contact::energy (src/ogc/potential.rs:39-65). Hessian-vector products are
+ * central differences of the exact FP64 gradient (largest displacement
+ * 1e-7 m) instead of assembled element Hessians. x_old, v_old: [n][3] in;
+ * x_out: [n][3] out. The solver's own state and history are not changed. */
+typedef struct cc_newton_report {
+    int32_t converged;
+    uint32_t iterations;             /* Newton iterations run                */
+    uint64_t pcg_iterations;         /* CG iterations over all solves        */
+    double residual_rms_n;           /* RMS gradient over free dofs at x_out */
+    double objective_j;              /* step objective at x_out              */
+    double relative_force_residual;  /* ||grad E(x_out)|| / ||grad E(y)||   */
+    uint64_t contact_terms;          /* frozen OGC contact terms             */
+} cc_newton_report;
+int32_t cc_solver_newton_step(cc_solver* solver, const double* x_old, const double* v_old,
+                              const cc_vbd_settings* settings, uint32_t newton_iterations,
+                              uint32_t pcg_iterations, double abs_tol, double rel_tol, double* x_out,
+                              cc_newton_report* report);
+
 /* ------------------------------------------------------------------ world */
 /* OgcWorld::new (src/ogc/world.rs:126-211). x: [n_all][3]; vertices >= moving
  * are fixed. excluded: [n_excluded][2] vertex pairs never in contact. */
