@@ -15,10 +15,10 @@
 // partial sums, and addition is commutative), so all lanes take identical
 // line-search decisions without a broadcast.
 //
-// All arithmetic is FP64: at cloth resolutions the in-plane membrane
-// stiffness per vertex (~1e5 N/m) is six to seven orders above the inertia
-// term (m/dt^2 ~ 1e-2 N/m), so an FP32 Hessian cannot represent the soft
-// (out-of-plane) direction that gravity acts along.
+// This is the FP64 form (cc_vbd_settings.sweep_precision = CC_SWEEP_FP64):
+// every term and the 3x3 solve in FP64, operation for operation as the CPU
+// path, so that GPU and CPU iterates agree to the last bits. sweep32.cu holds
+// the FP32-assembly form.
 #include "sweep_terms.cuh"
 
 namespace cc {
