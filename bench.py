@@ -241,6 +241,39 @@ def cpu_reference_run(sc, state, steps, budget_s, threads, warmup=0, warmup_budg
     return done, time.perf_counter() - t1, (its, force), warm
 
 
+BATCHED_STEPS = 5
+BATCHED_WARMUP = 2
+
+
+def batched_leg(rank, world, leg, L):
+    """Config 2 (96 uneven sheets with their own spheres, ~3.66M vertices,
+    20 fixed iterations): this rank's share of the instances as one batched
+    solver, BATCHED_WARMUP untimed steps (the first autotunes), then
+    BATCHED_STEPS device-timed steps; max over ranks."""
+    from clothcraft_b200 import scenes
+    from clothcraft_b200.batch import shard
+    from clothcraft_b200.vbd import VbdSolver
+
+    instances = scenes.config2_instances()
+    mine = shard(instances, rank, world)
+    solver = VbdSolver.batch([instances[i] for i in mine])
+    st = instances[0].settings.to_c()
+    for _ in range(BATCHED_WARMUP):
+        solver.step_resident(st)
+    ms, mets = leg(solver, lambda: solver.step_resident(st), BATCHED_STEPS)
+    vertices = sum(instances[i].n for i in mine)
+    total = sum(sc.n for sc in instances)
+    its = [int(m["iterations"]) for m in mets]
+    return {"workload": "config 2: %d sheets of 32..320 vertices a side (%d vertices in all), each with its own "
+                        "sphere, 1-4 pinned corners, moduli x U(0.5, 2); contact r 2 mm, 20 iterations"
+                        % (len(instances), total),
+            "steps": BATCHED_STEPS, "steps_per_s": BATCHED_STEPS / (ms / 1000.0), "ms_per_step": ms / BATCHED_STEPS,
+            "vertex_iters_per_s": world * vertices * sum(its) / (ms / 1000.0),
+            "vertices_per_rank": vertices, "instances_per_rank": len(mine),
+            "lanes": int(L.cc_solver_get_lanes(solver.h)),
+            "timing": "CUDA events on the solver stream, max over ranks; replicas shard the instances"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -278,6 +311,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances (config 2) leg")
     ap.add_argument("--lanes", type=int, default=0,
                     help="lanes per vertex solve (1..32); 0 = autotune on the first step")
     args = ap.parse_args()
@@ -476,6 +510,12 @@ def main():
                          "detection, colouring, learned guess and sweeps (predict, warm start, residual "
                          "checks, acceleration, commit, metrics)"}
 
+    # ---- batched uneven instances (config 2): 96 sheets, ~3.66M vertices, one
+    # solver per rank over its share (longest-first partition), 20 iterations
+    batched = None
+    if not args.no_batched:
+        batched = batched_leg(rank, world, leg, L)
+
     # ---- CPU baseline (rank 0, N=1 only): the oracle at equal residual from
     # the state the timed legs start from, a sample of about 30 s
     cpu = None
@@ -555,6 +595,7 @@ def main():
         "clocks": clocks.summary(),
         "detections_per_step": sum(m["detection_updates"] for m in mets_l) / K,
         "contact_terms_last": mets_l[-1]["contact_terms"] if mets_l else None,
+        "batched": batched,
     }
     print(json.dumps(line), flush=True)
     return 0
