@@ -426,6 +426,10 @@ def main():
     L.cc_solver_set_profiling(learned.h, 0)
     # ---- plain adaptive init at equal residual
     t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
+    # ---- the value leg's settings with each iteration chunk launched as a CUDA graph
+    graph_solver = make(1)
+    graph_solver.set_graphs(True)
+    t_g, mets_g = leg(graph_solver, lambda: graph_solver.step_resident(st_l), K)
     # ---- both inits at the other sweep precision (same target and acceleration)
     other = 1 - SWEEP_PRECISION
     other_legs = {}
@@ -551,6 +555,9 @@ def main():
         "learned_vs_plain_time_ratio": t_p / t_l,
         "learned_init_used_fraction": float(np.mean([m["init_used"] for m in mets_l])),
         "acceleration": ACCELERATION,
+        "graphs": dict(summary(t_g, mets_g), note="the learned leg with every iteration chunk captured into a "
+                                                   "CUDA graph and launched as one (updated in place while its "
+                                                   "topology holds)"),
         "sweep_precision": ("fp32 element assembly" if SWEEP_PRECISION else "fp64"),
         "other_precision": {"sweep_precision": ("fp32 element assembly" if other else "fp64"),
                             "learned": summary(*other_legs[1]), "plain": summary(*other_legs[0]),
@@ -590,7 +597,10 @@ def main():
                 "host_memory": "pinned, [n][3] float64 x and v, stepped in place (VbdSolver.step_into)"},
         "gpu_launches": int(sum(m["kernel_launches"] for m in mets_l)),
         "lanes_per_vertex": int(L.cc_solver_get_lanes(learned.h)) & 0xff,
-        "blocks_per_sm_cap": int(L.cc_solver_get_lanes(learned.h)) >> 8,
+        "blocks_per_sm_cap": (int(L.cc_solver_get_lanes(learned.h)) >> 8) & 0xff,
+        "sweep_variant": {"encoded": int(L.cc_solver_get_lanes(learned.h)),
+                          "persistent_grid": bool(int(L.cc_solver_get_lanes(learned.h)) & (1 << 16)),
+                          "block_threads": {0: 128, 1: 64, 2: 256}[(int(L.cc_solver_get_lanes(learned.h)) >> 17) & 3]},
         "breakdown_ms_per_step": breakdown,
         "clocks": clocks.summary(),
         "detections_per_step": sum(m["detection_updates"] for m in mets_l) / K,

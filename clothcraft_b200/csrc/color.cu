@@ -232,7 +232,7 @@ void Coloring::compute(const ColorView& view, cudaStream_t s) {
     // colour does not change any result (no two vertices of a colour interact).
     int bits = 1;
     while ((1u << bits) < n_colors_) ++bits;
-    launches_ += sorter_.sort_pairs(cur_, b_.ptr, iota_.ptr, order_.ptr, n, bits, s);
+    launches_ += sorter_.sort_pairs(cur_, b_.ptr, iota_.ptr, order_.ptr, n, bits, s, error_word_, DERR_SORT_WAIT);
     CC_CUDA(cudaGetLastError());
 }
 

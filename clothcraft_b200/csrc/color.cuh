@@ -24,6 +24,8 @@ class Coloring {
     const std::vector<uint32_t>& offsets() const { return offsets_h_; }
     const uint32_t* order() const { return order_.ptr; }
     const uint16_t* colors() const { return cur_; }
+    // device word that receives DERR_SORT_WAIT if the colour sort's wait gives up
+    void set_error_word(unsigned int* w) { error_word_ = w; }
     size_t last_iterations() const { return last_iterations_; }
     void download(std::vector<uint32_t>& colors);
     uint64_t launches() const { return launches_; }
@@ -35,6 +37,7 @@ class Coloring {
     uint16_t* cur_ = nullptr;
     DBuf<uint32_t> order_, counts_, iota_;
     RadixSorter sorter_;
+    unsigned int* error_word_ = nullptr;  // receives DERR_SORT_WAIT (set_error_word)
     DBuf<unsigned int> changed_;
     Pinned<unsigned int> changed_h_;
     Pinned<uint32_t> counts_h_;

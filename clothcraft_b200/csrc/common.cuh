@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
@@ -41,6 +42,7 @@ enum DeviceError : uint32_t {
     DERR_TRUST_REGION = 1u << 5,
     DERR_COLOR_LIMIT = 1u << 6,
     DERR_INTERSECTION = 1u << 7,
+    DERR_SORT_WAIT = 1u << 8,  // a radix-sort look-back wait gave up
 };
 
 // ------------------------------------------------------------ device buffer
@@ -148,6 +150,19 @@ template <class K>
 inline void allow_dynamic_smem(K* kernel, size_t bytes) {
     if (bytes > 48 * 1024)
         CC_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// The same for a kernel launched many times per step: `raised` records, one
+// bit per device (ids below 64), where the limit is already raised, so the
+// attribute is set once per device instead of before every launch.
+template <class K>
+inline void allow_dynamic_smem_once(K* kernel, size_t bytes, std::atomic<uint64_t>& raised) {
+    int dev = 0;
+    CC_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = dev >= 0 && dev < 64 ? (1ull << dev) : 0ull;
+    if (bit && (raised.load(std::memory_order_acquire) & bit)) return;
+    allow_dynamic_smem(kernel, bytes);
+    if (bit) raised.fetch_or(bit, std::memory_order_acq_rel);
 }
 
 inline int grid_for(size_t n, int block) {

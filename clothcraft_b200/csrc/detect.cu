@@ -202,7 +202,7 @@ __global__ void k_lbvh_boxes(const Box* prim_box, const uint32_t* leaf_prim, int
     }
 }
 
-int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaStream_t s) {
+int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaStream_t s, unsigned int* err) {
     m = count;
     if (m == 0) return 0;
     leaf_prim.reserve(m);
@@ -218,7 +218,7 @@ int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaSt
     k_bounds_init<<<1, 32, 0, s>>>(bounds.ptr);
     k_centroid_bounds<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr);
     k_morton<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr, morton_tmp.ptr, ids_tmp.ptr);
-    int sorts = sorter.sort_pairs(morton_tmp.ptr, morton.ptr, ids_tmp.ptr, leaf_prim.ptr, m, 63, s);
+    int sorts = sorter.sort_pairs(morton_tmp.ptr, morton.ptr, ids_tmp.ptr, leaf_prim.ptr, m, 63, s, err, DERR_SORT_WAIT);
     if (m > 1) {
         k_karras<<<grid_for(m - 1, 256), 256, 0, s>>>(morton.ptr, (int)m, child.ptr, parent.ptr);
         CC_CUDA(cudaMemsetAsync(visits.ptr, 0, (m - 1) * sizeof(unsigned), s));
@@ -993,8 +993,8 @@ World::World(const double* x_all, size_t n_all, const std::vector<std::array<uin
     // fixed trees are built once: fixed geometry never moves
     stats_d_.zero(1, stream_);
     refit(false);
-    tree_tri_fixed_.build(tri_box_.ptr, tri_fixed_.ptr, (uint32_t)tri_fixed_h_.size(), stream_);
-    tree_edge_fixed_.build(edge_box_.ptr, edge_fixed_.ptr, (uint32_t)edge_fixed_h_.size(), stream_);
+    tree_tri_fixed_.build(tri_box_.ptr, tri_fixed_.ptr, (uint32_t)tri_fixed_h_.size(), stream_, &stats_d_.ptr->error);
+    tree_edge_fixed_.build(edge_box_.ptr, edge_fixed_.ptr, (uint32_t)edge_fixed_h_.size(), stream_, &stats_d_.ptr->error);
     CC_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -1044,13 +1044,14 @@ static void raise_device_error(unsigned int e) {
     if (e & DERR_FIXED_MOVED) throw Failure{CC_ERR_INVALID_STATE, "OGC fixed geometry changed; rebuild the world"};
     if (e & DERR_DEGENERATE_FACE) throw Failure{CC_ERR_CONTACT, "OGC degenerate face; step rejected"};
     if (e & DERR_STACK_OVERFLOW) throw Failure{CC_ERR_CUDA, "OGC LBVH traversal stack overflow"};
+    if (e & DERR_SORT_WAIT) throw Failure{CC_ERR_DEVICE_TIMEOUT, "OGC radix sort look-back wait gave up"};
 }
 
 void World::build_candidates(double R, double skin) {
     double search = R + 2.0 * skin + 1e-12;  // candidates.rs:23-28
     double search2 = search * search;
-    launches_ += tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_);
-    launches_ += tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_);
+    launches_ += tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_, &stats_d_.ptr->error);
+    launches_ += tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_, &stats_d_.ptr->error);
     LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
     LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
     if (vf_cap_ == 0) {
@@ -1190,11 +1191,11 @@ void World::detect(double query_radius, double radius, double relaxation, double
         uniq_pos_.reserve(n_raw);
         const int lo_bits = (int)(2 * nb), hi_bits = (int)(2 * nb + 2);
         launches_ += sorter_.sort_pairs(raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_idx_s_.ptr, n_raw, lo_bits,
-                                        stream_);
+                                        stream_, &sd->error, DERR_SORT_WAIT);
         // gather hi in lo order, then stable sort by hi
         k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_idx_s_.ptr, raw_hi_s_.ptr, n_raw);
         launches_ += sorter_.sort_pairs(raw_hi_s_.ptr, raw_hi_.ptr, raw_idx_s_.ptr, raw_idx_.ptr, n_raw, hi_bits,
-                                        stream_);
+                                        stream_, &sd->error, DERR_SORT_WAIT);
         // raw_hi_ = sorted hi, raw_idx_ = original index; gather lo
         k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_lo_.ptr, raw_idx_.ptr, raw_lo_s_.ptr, n_raw);
         k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, n_raw, uniq_flag_.ptr);
@@ -1255,7 +1256,7 @@ void World::validate_start() {  // world.rs:242-307
     unsigned long long none = ~0ull;
     CC_CUDA(cudaMemcpyAsync(&stats_d_.ptr->intersect_key, &none, 8, cudaMemcpyHostToDevice, stream_));
     refit(true);
-    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_);
+    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_, &stats_d_.ptr->error);
     k_intersections<<<grid_for(n_tri_, 128), 128, 0, stream_>>>(view(), tree_tri_moving_.view(tri_box_.ptr),
                                                                 tree_tri_fixed_.view(tri_box_.ptr), nullptr,
                                                                 &stats_d_.ptr->intersect_key, &stats_d_.ptr->error);
@@ -1291,8 +1292,8 @@ void World::fresh_pairs(double search, std::vector<uint32_t>& vf, std::vector<ui
     // exact search radius: build_candidates adds 2*skin + 1e-12, so pass R
     // such that the sum equals `search`
     double search2 = search * search;
-    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_);
-    tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_);
+    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_, &stats_d_.ptr->error);
+    tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_, &stats_d_.ptr->error);
     LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
     LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
     size_t vcap = std::max<size_t>(1024, 16 * n_all_), ecap = std::max<size_t>(1024, 32 * n_edge_);

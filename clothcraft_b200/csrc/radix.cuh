@@ -1,16 +1,17 @@
 // The library's own device sort and scans: a stable LSD radix sort of
 // (key, value) pairs with 8-bit digits, and exclusive / inclusive prefix sums.
 //
-// Each radix pass is three kernels and needs no block to wait on another:
-//   upsweep   - per tile of 2048 keys, the histogram of the pass's digit,
-//               stored digit-major ([digit][tile]);
-//   scan      - one block turns the histograms into exclusive global offsets
-//               (digit-major order = where each tile's keys of a digit go);
-//   downsweep - per tile, the stable rank of every key among the tile's keys
-//               of the same digit (warp match + per-warp digit counts, in
-//               index order), then the scatter to offset + rank.
-// The sort is stable, so an LSD sequence of passes orders by the whole key
-// and keeps equal keys in input order; the inputs are left untouched.
+// The sort reads every key once for the digit histograms of all its passes,
+// then runs one kernel per pass: each block takes the next tile of 2048 keys
+// (tiles numbered in the order blocks start), ranks them stably among the
+// tile's keys of the same digit (warp match in index order, per-warp digit
+// counts across warps), publishes the tile's digit counts and adds its
+// predecessors' counts by looking back through their published words
+// (decoupled look-back), then scatters. A block only ever waits on blocks
+// that started before it, and each wait is bounded: a look-back that gives
+// up sets an error bit in the caller's error word instead of hanging.
+// Stability keeps equal keys in input order, so the passes order by the whole
+// key; the inputs are left untouched.
 #pragma once
 #include "common.cuh"
 
@@ -21,12 +22,14 @@ class RadixSorter {
     // keys_out/vals_out[i] = the pairs of keys_in/vals_in ordered by the low
     // `bits` bits of the key (stable). K: uint16_t, uint32_t or uint64_t;
     // V: uint32_t or double. Returns the number of kernels launched.
+    // `err` (device, may be null) receives `err_bit` if a look-back wait gave up.
     template <class K, class V>
     int sort_pairs(const K* keys_in, K* keys_out, const V* vals_in, V* vals_out, size_t n, int bits,
-                   cudaStream_t s);
+                   cudaStream_t s, unsigned int* err = nullptr, unsigned int err_bit = 1u);
 
    private:
     DBuf<uint32_t> hist_;
+    DBuf<unsigned int> err_;
     DBuf<unsigned char> keys_tmp_, vals_tmp_;
 };
 

@@ -7,6 +7,7 @@
 // kernels and reads a few scalars between phases.
 #include <chrono>
 #include <cmath>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <set>
@@ -509,6 +510,7 @@ struct cc_solver {
         if (learn0) cudaEventDestroy(learn0);
         if (learn1) cudaEventDestroy(learn1);
         for (auto e : prof_events) cudaEventDestroy(e);
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -586,11 +588,53 @@ struct cc_solver {
         }
     }
 
+    // CUDA-graph launch of the iteration chunks (cc_solver_set_graphs)
+    bool graphs = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_instantiations = 0, graph_updates = 0;
+    void launch_captured_chunk() {
+        cudaGraph_t g = nullptr;
+        CC_CUDA(cudaStreamEndCapture(stream, &g));
+        if (graph_exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(graph_exec, g, &info) == cudaSuccess) {
+                ++graph_updates;
+            } else {
+                (void)cudaGetLastError();  // a topology change: not an error
+                cudaGraphExecDestroy(graph_exec);
+                graph_exec = nullptr;
+            }
+        }
+        if (!graph_exec) {
+            cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+            if (e != cudaSuccess) {
+                cudaGraphDestroy(g);
+                graph_exec = nullptr;
+                cuda_check(e, "cudaGraphInstantiate");
+            }
+            ++graph_instantiations;
+        }
+        CC_CUDA(cudaGraphDestroy(g));
+        CC_CUDA(cudaGraphLaunch(graph_exec, stream));
+    }
     void step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out);
     void autotune(const SweepView& sv, bool fp32);
+    std::map<int, unsigned> resident_;  // resident blocks of each variant's kernel (fp32 variants | 1 << 30)
+    unsigned grid_cap(int variant, bool fp32) {
+        if (!(variant & kVariantPersistent)) return 0;
+        int key = variant | (fp32 ? 1 << 30 : 0);
+        auto it = resident_.find(key);
+        if (it != resident_.end()) return it->second;
+        unsigned r = fp32 ? sweep32_resident_blocks(variant) : sweep_resident_blocks(variant);
+        resident_[key] = r;
+        return r;
+    }
+    void launch_variant(const SweepView& sv, const uint32_t* order, uint32_t count, int variant, bool fp32) {
+        if (fp32) launch_sweep32(sv, order, count, variant, stream, grid_cap(variant, true));
+        else launch_sweep(sv, order, count, variant, stream, grid_cap(variant, false));
+    }
     void sweep(const SweepView& sv, const uint32_t* order, uint32_t count, bool fp32) {
-        if (fp32) launch_sweep32(sv, order, count, lanes32, stream);
-        else launch_sweep(sv, order, count, lanes, stream);
+        launch_variant(sv, order, count, fp32 ? lanes32 : lanes, fp32);
     }
     ObjectiveCounts counts() const {
         return ObjectiveCounts{n_tri, n_hinge, n_stitch, world->stats().n_contacts};
@@ -644,6 +688,7 @@ struct cc_solver {
     }
     void color(const ContactsView& cv, const cc_grab* grab, cc_metrics& m) {
         double t = now_ms();
+        coloring.set_error_word(&sc.ptr->error);
         coloring.compute(color_view(cv, grab), stream);
         m.color_ms += now_ms() - t;
         m.color_rounds += coloring.last_iterations();
@@ -655,12 +700,20 @@ struct cc_solver {
 void cc_solver::autotune(const SweepView& sv_in, bool fp32) {
     // lanes per vertex | register cap (resident 128-thread blocks per SM: 3, 4, 5,
     // 6 or 8; above 3 the compiler spills to local memory) << 8
-    static const int kCandidates64[] = {1 | 3 << 8,  2 | 3 << 8,  4 | 3 << 8,  4 | 4 << 8,  4 | 5 << 8,  4 | 6 << 8,
-                                        8 | 3 << 8,  8 | 4 << 8,  8 | 5 << 8,  8 | 6 << 8,  8 | 8 << 8,  16 | 3 << 8,
-                                        16 | 4 << 8, 16 | 6 << 8, 16 | 8 << 8, 32 | 3 << 8};
-    static const int kCandidates32[] = {4 | 3 << 8,  4 | 4 << 8,  8 | 3 << 8,  8 | 4 << 8,  8 | 5 << 8,
-                                        8 | 6 << 8,  8 | 8 << 8,  16 | 3 << 8, 16 | 4 << 8, 16 | 6 << 8,
-                                        16 | 8 << 8, 32 | 3 << 8, 32 | 4 << 8};
+    // | kVariantPersistent: a grid of the resident blocks looping over the colour;
+    // | 1 << 17 or 2 << 17: blocks of 64 or 256 threads at the same register budget
+    constexpr int P = kVariantPersistent, B64 = 1 << 17, B256 = 2 << 17;
+    static const int kCandidates64[] = {1 | 3 << 8,      2 | 3 << 8,       4 | 3 << 8,      4 | 4 << 8,
+                                        4 | 5 << 8,      4 | 6 << 8,       8 | 3 << 8,      8 | 4 << 8,
+                                        8 | 5 << 8,      8 | 6 << 8,       8 | 8 << 8,      16 | 3 << 8,
+                                        16 | 4 << 8,     16 | 6 << 8,      16 | 8 << 8,     32 | 3 << 8,
+                                        4 | 4 << 8 | P,  8 | 4 << 8 | P,   8 | 3 << 8 | P,  4 | 4 << 8 | B64,
+                                        8 | 4 << 8 | B64, 8 | 4 << 8 | B256, 4 | 4 << 8 | B256, 8 | 4 << 8 | B64 | P};
+    static const int kCandidates32[] = {4 | 3 << 8,       4 | 4 << 8,        8 | 3 << 8,      8 | 4 << 8,
+                                        8 | 5 << 8,       8 | 6 << 8,        8 | 8 << 8,      16 | 3 << 8,
+                                        16 | 4 << 8,      16 | 6 << 8,       16 | 8 << 8,     32 | 3 << 8,
+                                        32 | 4 << 8,      8 | 4 << 8 | P,    16 | 4 << 8 | P, 8 | 4 << 8 | B64,
+                                        16 | 4 << 8 | B64, 8 | 4 << 8 | B256, 16 | 4 << 8 | B256};
     const int* cands = fp32 ? kCandidates32 : kCandidates64;
     const size_t n_cands = fp32 ? sizeof(kCandidates32) / sizeof(int) : sizeof(kCandidates64) / sizeof(int);
     SweepView sv = sv_in;  // trial sweeps never skip and count into a scratch counter
@@ -678,10 +731,8 @@ void cc_solver::autotune(const SweepView& sv_in, bool fp32) {
         for (int rep = 0; rep < 4; ++rep) {  // first repetition warms caches; keep the fastest of the rest
             CC_CUDA(cudaEventRecord(tune0, stream));
             for (int sweep = 0; sweep < 2; ++sweep)  // two consecutive sweeps, as the iterations run
-                for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
-                    if (fp32) launch_sweep32(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
-                    else launch_sweep(sv, coloring.order() + off[c], off[c + 1] - off[c], g, stream);
-                }
+                for (uint32_t c = 0; c < coloring.n_colors(); ++c)
+                    launch_variant(sv, coloring.order() + off[c], off[c + 1] - off[c], g, fp32);
             CC_CUDA(cudaEventRecord(tune1, stream));
             CC_CUDA(cudaMemcpyAsync(world->x(), x_backup.ptr, n * sizeof(double4), cudaMemcpyDeviceToDevice, stream));
             CC_CUDA(cudaEventSynchronize(tune1));
@@ -864,8 +915,15 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         size_t batch_first_pair = prof_pairs.size();
         const uint32_t chunk = target_on ? std::max<uint32_t>(check_every, 4) : s.iterations;
         uint32_t chunks = 0;
+        // graph mode: each chunk's launches are captured into a CUDA graph; the
+        // executable graph is updated in place while the chunk's topology (the
+        // colour count and the placement of the residual checks) stays the
+        // same, and instantiated anew when it changes
+        const bool capture = graphs && !profiling;
         for (uint32_t c0 = it0; c0 < s.iterations; c0 += chunk) {
             uint32_t c1 = std::min(s.iterations, c0 + chunk);
+            if (capture) CC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+            try {
             for (uint32_t it = c0; it < c1; ++it) {
                 sv.iteration = it;
                 sv.clipped = &sc.ptr->clipped_iter[it];
@@ -905,6 +963,15 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                     own_launches += 3;
                 }
             }
+            } catch (...) {
+                if (capture) {  // leave the stream out of capture mode before the failure propagates
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                }
+                throw;
+            }
+            if (capture) launch_captured_chunk();
             CC_CUDA(cudaGetLastError());
             if (c1 >= s.iterations || !target_on) break;
             // look ahead: enqueue the next chunk before waiting on this one's stop flag
@@ -964,6 +1031,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     ++own_launches;
     CC_CUDA(cudaGetLastError());
     read_scalars();
+    if (sc_h.ptr->error & DERR_SORT_WAIT)
+        throw Failure{CC_ERR_DEVICE_TIMEOUT, "colour sort look-back wait gave up; state unchanged"};
     if (sc_h.ptr->error & DERR_NONFINITE_RESULT) throw Failure{CC_ERR_NON_FINITE, "Non-finite VBD result; state unchanged"};
     if (checks) m.relative_force_residual = std::sqrt(sc_h.ptr->gx2_plain / sc_h.ptr->gy2);
     if (sc_h.ptr->error & DERR_TRUST_REGION) throw Failure{CC_ERR_CONTACT, "OGC trust-region invariant failed"};
@@ -986,7 +1055,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         k_stretch<<<grid_for(n_tri, 256), 256, 0, stream>>>(n_tri, tri_v.ptr, tri_coef.ptr, tri_area.ptr, x0.ptr,
                                                             ext_key.ptr, ext_w.ptr);
         own_launches += 2;  // k_stretch and k_p95
-        own_launches += ext_sorter.sort_pairs(ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr, n_tri, 64, stream);
+        own_launches += ext_sorter.sort_pairs(ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr, n_tri, 64, stream,
+                                              &sc.ptr->error, DERR_SORT_WAIT);
         own_launches += inclusive_sum(ext_w_s.ptr, ext_cum.ptr, n_tri, ext_scan, stream);
         double total = 0.0;
         unsigned long long kmax = 0, kp = order_key(0.0);
@@ -1002,6 +1072,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     }
     CC_CUDA(cudaEventRecord(ev1, stream));
     read_scalars();
+    const bool metric_sort_failed = (sc_h.ptr->error & DERR_SORT_WAIT) != 0;  // the step is committed already
     float gms = 0.f;
     CC_CUDA(cudaEventElapsedTime(&gms, ev0, ev1));
     double gap;
@@ -1015,8 +1086,8 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         std::memcpy(&m.minimum_distance_m, &b, 8);
     }
     m.max_seam_gap_m = n_stitch ? gap : 0.0;
-    m.extension_p95_percent = p95;
-    m.extension_max_percent = emax;
+    m.extension_p95_percent = metric_sort_failed ? std::nan("") : p95;
+    m.extension_max_percent = metric_sort_failed ? std::nan("") : emax;
     m.detection_ms = det_ms;
     m.gpu_compute_ms = gms;
     if (profiling) {
@@ -1327,29 +1398,40 @@ void cc_solver_destroy(cc_solver* s) { delete s; }
 uint64_t cc_solver_moving(const cc_solver* s) { return s->n; }
 uint64_t cc_solver_total(const cc_solver* s) { return s->n_all; }
 void* cc_solver_stream(const cc_solver* s) { return (void*)s->stream; }
+int32_t cc_solver_set_graphs(cc_solver* s, int32_t enable) {
+    s->graphs = enable != 0;
+    return CC_OK;
+}
 int32_t cc_solver_set_profiling(cc_solver* s, int32_t enable) {
     s->profiling = enable != 0;
     return CC_OK;
 }
+// 0, or a sweep variant with the cap defaulting to 3
+static int normalize_variant(int32_t v) {
+    if (v == 0) return 0;
+    if (((v >> 8) & 0xff) == 0) v |= 3 << 8;
+    return v;
+}
+
 int32_t cc_solver_set_lanes(cc_solver* s, int32_t lanes) {
-    int32_t g = lanes & 0xff, cap = lanes >> 8;
-    if (!(g == 0 || g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) ||
-        !(cap == 0 || cap == 3 || cap == 4 || cap == 5 || cap == 6 || cap == 8) || (g == 0 && cap != 0))
+    int v = normalize_variant(lanes);
+    if (v != 0 && !sweep_variant_valid(v, false))
         return s->fail(Failure{CC_ERR_INVALID_ARGUMENT,
                                "lanes must be 0 (autotune) or a power of two up to 32, optionally | cap << 8 with "
-                               "cap 3, 4, 5, 6 or 8"});
-    s->lanes = lanes == 0 ? 0 : (g | (cap ? cap : 3) << 8);
+                               "cap 3, 4, 5, 6 or 8, | 1 << 16 (persistent grid), | 1 << 17 or 2 << 17 (64- or "
+                               "256-thread blocks, 4 or 8 lanes)"});
+    s->lanes = v;
     return CC_OK;
 }
 int32_t cc_solver_get_lanes(const cc_solver* s) { return s->lanes; }
 int32_t cc_solver_set_lanes32(cc_solver* s, int32_t lanes) {
-    int32_t g = lanes & 0xff, cap = lanes >> 8;
-    if (!(g == 0 || g == 4 || g == 8 || g == 16 || g == 32) ||
-        !(cap == 0 || cap == 3 || cap == 4 || cap == 5 || cap == 6 || cap == 8) || (g == 0 && cap != 0))
+    int v = normalize_variant(lanes);
+    if (v != 0 && !sweep_variant_valid(v, true))
         return s->fail(Failure{CC_ERR_INVALID_ARGUMENT,
                                "FP32 sweep lanes must be 0 (autotune), 4, 8, 16 or 32, optionally | cap << 8 "
-                               "with cap 3, 4, 5, 6 or 8"});
-    s->lanes32 = lanes == 0 ? 0 : (g | (cap ? cap : 3) << 8);
+                               "with cap 3, 4, 5, 6 or 8, | 1 << 16 (persistent grid), | 1 << 17 or 2 << 17 "
+                               "(64- or 256-thread blocks, 8 or 16 lanes)"});
+    s->lanes32 = v;
     return CC_OK;
 }
 int32_t cc_solver_get_lanes32(const cc_solver* s) { return s->lanes32; }

@@ -89,42 +89,114 @@ __device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uin
 }
 
 // MINB blocks of BLOCK threads per SM caps the registers (65536 / (MINB*BLOCK)).
+// Each group of G lanes solves vertices gi, gi + groups in the grid, ...: one
+// vertex per group when the grid covers the colour, several in a persistent grid.
 template <int G, int BLOCK, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_sweep(SweepView s, const uint32_t* order, uint32_t count) {
     if (s.skip_at && *s.skip_at <= s.iteration) return;  // a refresh detection precedes this iteration
-    uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
-    uint32_t gi = t / G;
-    if (gi >= count) return;  // whole groups leave together
-    uint32_t lane = threadIdx.x & (G - 1);
-    unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
-    solve_vertex<G>(s, order[gi], lane, mask);
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
+    constexpr uint32_t kGroups = BLOCK / G;
+    // whole groups step together
+    for (uint32_t gi = blockIdx.x * kGroups + threadIdx.x / G; gi < count; gi += gridDim.x * kGroups)
+        solve_vertex<G>(s, order[gi], lane, mask);
 }
 
-template <int G>
-static void launch_g(const SweepView& s, const uint32_t* order, uint32_t count, int minb, cudaStream_t st) {
-    constexpr int B = 128;
+template <int G, int B, int MINB>
+static void launch_k(const SweepView& s, const uint32_t* order, uint32_t count, cudaStream_t st, unsigned cap) {
     uint64_t threads = (uint64_t)count * G;
     unsigned grid = (unsigned)((threads + B - 1) / B);
-    if (minb >= 8) k_sweep<G, B, 8><<<grid, B, 0, st>>>(s, order, count);
-    else if (minb >= 6) k_sweep<G, B, 6><<<grid, B, 0, st>>>(s, order, count);
-    else if (minb == 5) k_sweep<G, B, 5><<<grid, B, 0, st>>>(s, order, count);
-    else if (minb == 4) k_sweep<G, B, 4><<<grid, B, 0, st>>>(s, order, count);
-    else k_sweep<G, B, 3><<<grid, B, 0, st>>>(s, order, count);
+    if (cap && grid > cap) grid = cap;
+    k_sweep<G, B, MINB><<<grid, B, 0, st>>>(s, order, count);
 }
 
-// variant = lanes per vertex (1..32) | occupancy cap (blocks per SM) << 8
-void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st) {
-    if (count == 0) return;
-    int lanes = variant & 0xff, minb = variant >> 8;
-    switch (lanes) {
-        case 1: launch_g<1>(s, order, count, minb, st); break;
-        case 2: launch_g<2>(s, order, count, minb, st); break;
-        case 4: launch_g<4>(s, order, count, minb, st); break;
-        case 16: launch_g<16>(s, order, count, minb, st); break;
-        case 32: launch_g<32>(s, order, count, minb, st); break;
-        default: launch_g<8>(s, order, count, minb, st); break;
+template <int G, int B, int MINB>
+static unsigned resident_k() {
+    int dev = 0, sms = 0, per = 0;
+    CC_CUDA(cudaGetDevice(&dev));
+    CC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweep<G, B, MINB>, B, 0));
+    return (unsigned)(sms * (per > 0 ? per : 1));
+}
+
+// Dispatch of (lanes, cap, block) to a kernel instance; F(G, B, MINB) is
+// called for the instance. Blocks of 64 and 256 threads exist for 4 and 8
+// lanes at the register budgets of caps 3-4 (64) and 4, 6, 8 (256).
+template <int G, class F>
+static auto dispatch_cap(const SweepVariant& v, F&& f) {
+    if (v.block == 64) {
+        if (v.cap >= 4) return f.template operator()<G, 64, 8>();
+        return f.template operator()<G, 64, 6>();
+    }
+    if (v.block == 256) {
+        if (v.cap >= 8) return f.template operator()<G, 256, 4>();
+        if (v.cap >= 6) return f.template operator()<G, 256, 3>();
+        return f.template operator()<G, 256, 2>();
+    }
+    if (v.cap >= 8) return f.template operator()<G, 128, 8>();
+    if (v.cap >= 6) return f.template operator()<G, 128, 6>();
+    if (v.cap == 5) return f.template operator()<G, 128, 5>();
+    if (v.cap == 4) return f.template operator()<G, 128, 4>();
+    return f.template operator()<G, 128, 3>();
+}
+
+template <class F>
+static auto dispatch(const SweepVariant& v, F&& f) {
+    switch (v.lanes) {
+        case 1: return dispatch_cap<1>(SweepVariant{1, v.cap, 128, v.persistent}, f);
+        case 2: return dispatch_cap<2>(SweepVariant{2, v.cap, 128, v.persistent}, f);
+        case 4: return dispatch_cap<4>(v, f);
+        case 16: return dispatch_cap<16>(SweepVariant{16, v.cap, 128, v.persistent}, f);
+        case 32: return dispatch_cap<32>(SweepVariant{32, v.cap, 128, v.persistent}, f);
+        default: return dispatch_cap<8>(v, f);
     }
 }
+
+bool sweep_variant_valid(int variant, bool fp32) {
+    if (variant & ~((1 << 19) - 1)) return false;
+    SweepVariant v = decode_variant(variant);
+    int code = (variant >> 17) & 3;
+    if (code == 3) return false;
+    bool cap_ok = v.cap == 3 || v.cap == 4 || v.cap == 5 || v.cap == 6 || v.cap == 8;
+    bool lanes_ok = fp32 ? (v.lanes == 4 || v.lanes == 8 || v.lanes == 16 || v.lanes == 32)
+                         : (v.lanes == 1 || v.lanes == 2 || v.lanes == 4 || v.lanes == 8 || v.lanes == 16 ||
+                            v.lanes == 32);
+    if (!cap_ok || !lanes_ok) return false;
+    if (v.block == 128) return true;
+    bool wide = fp32 ? (v.lanes == 8 || v.lanes == 16) : (v.lanes == 4 || v.lanes == 8);
+    if (!wide) return false;
+    return v.block == 64 ? (v.cap == 3 || v.cap == 4) : (v.cap == 4 || v.cap == 6 || v.cap == 8);
+}
+
+namespace {
+struct SweepLaunch {
+    const SweepView& s;
+    const uint32_t* order;
+    uint32_t count;
+    cudaStream_t st;
+    unsigned cap;
+    template <int G, int B, int MINB>
+    int operator()() const {
+        launch_k<G, B, MINB>(s, order, count, st, cap);
+        return 0;
+    }
+};
+struct SweepResident {
+    template <int G, int B, int MINB>
+    unsigned operator()() const {
+        return resident_k<G, B, MINB>();
+    }
+};
+}  // namespace
+
+void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st,
+                  unsigned grid_cap) {
+    if (count == 0) return;
+    SweepVariant v = decode_variant(variant);
+    dispatch(v, SweepLaunch{s, order, count, st, v.persistent ? grid_cap : 0u});
+}
+
+unsigned sweep_resident_blocks(int variant) { return dispatch(decode_variant(variant), SweepResident{}); }
 
 // Probe: local e, g, H of every moving vertex at the current positions
 // (the f64 gradient check of src/gpu_vbd.rs:305-379, probe of vbd.wgsl:142-147).

@@ -64,10 +64,32 @@ __host__ __device__ inline uint64_t objective_items(const ObjectiveCounts& c) {
 }
 constexpr int kSumBlocks = 296;  // 2 x 148 SMs
 
-// launch helpers (sweep.cu)
-void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
-// FP32 element assembly (sweep32.cu); lanes 4, 8, 16 or 32 | cap << 8
-void launch_sweep32(const SweepView& s, const uint32_t* order, uint32_t count, int lanes, cudaStream_t st);
+// Sweep variant (an int): lanes per vertex (bits 0-7) | cap (bits 8-15: resident
+// 128-thread blocks per SM the registers are budgeted for) | kVariantPersistent
+// (bit 16: a grid of at most the resident blocks, each block looping over the
+// colour's vertices) | block-size code << 17 (0: 128 threads, 1: 64, 2: 256;
+// the register budget per thread stays that of `cap` 128-thread blocks).
+constexpr int kVariantPersistent = 1 << 16;
+struct SweepVariant {
+    int lanes, cap, block;
+    bool persistent;
+};
+inline SweepVariant decode_variant(int v) {
+    int code = (v >> 17) & 3;
+    return {v & 0xff, (v >> 8) & 0xff, code == 1 ? 64 : (code == 2 ? 256 : 128), (v & kVariantPersistent) != 0};
+}
+// valid variants of the FP64 (fp32 = false) and FP32-assembly sweeps
+bool sweep_variant_valid(int v, bool fp32);
+
+// launch helpers (sweep.cu); grid_cap > 0 limits the grid (persistent variants)
+void launch_sweep(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st,
+                  unsigned grid_cap = 0);
+// FP32 element assembly (sweep32.cu); lanes 4, 8, 16 or 32
+void launch_sweep32(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st,
+                    unsigned grid_cap = 0);
+// resident blocks of a variant's kernel on the current device (all SMs)
+unsigned sweep_resident_blocks(int variant);
+unsigned sweep32_resident_blocks(int variant);
 void launch_local_blocks(const SweepView& s, double* energy, double* grad, double* hess, cudaStream_t st);
 // out[v] = |dE/dx_v|^2 over moving vertices (variant as launch_sweep); with
 // `project`, the KKT residual of the OGC-ball constraints (sweep.cu)

@@ -23,6 +23,8 @@
 // up to ten trial evaluations read no global memory for membrane and bending
 // terms. A lane's terms beyond the staging slots are recomputed from global
 // memory in each trial.
+#include <atomic>
+
 #include "sweep_terms.cuh"
 
 namespace cc {
@@ -86,14 +88,20 @@ __device__ __forceinline__ TriRec tri_rec(const SweepView& s, uint32_t t, uint32
     d3 x0 = slot == 0 ? x : ld3(s.x, (uint32_t)tv.x);
     d3 x1 = slot == 1 ? x : ld3(s.x, (uint32_t)tv.y);
     d3 x2 = slot == 2 ? x : ld3(s.x, (uint32_t)tv.z);
-    f3 ds0 = tof(x1 - x0), ds1 = tof(x2 - x0);  // FP64 differences, rounded once
+    // The Green strains are formed in FP64 from the FP64 edge differences and
+    // rounded once: 1/2 (w.w - 1) cancels to ~1e-4 of its terms, so an FP32
+    // strain would carry ~1e-7 of absolute error, a force noise that left the
+    // relative force residual of the 64x64 sheet on a sphere at ~0.19 after
+    // 100 steps (FP64: 0.068). Everything after that is FP32.
+    const d3 e0 = x1 - x0, e1 = x2 - x0;
+    const d3 w64 = e0 * cf.x + e1 * cf.y, v64 = e0 * cf.z + e1 * cf.w;
     float cx = (float)cf.x, cy = (float)cf.y, cz = (float)cf.z, cw = (float)cf.w;
     TriRec r;
-    r.w = ds0 * cx + ds1 * cy;
-    r.v = ds0 * cz + ds1 * cw;
-    r.ew = 0.5f * (fdot(r.w, r.w) - 1.f);
-    r.ev = 0.5f * (fdot(r.v, r.v) - 1.f);
-    r.sh = fdot(r.w, r.v);
+    r.w = tof(w64);
+    r.v = tof(v64);
+    r.ew = (float)((dot(w64, w64) - 1.0) * 0.5);
+    r.ev = (float)((dot(v64, v64) - 1.0) * 0.5);
+    r.sh = (float)dot(w64, v64);
     r.aw = slot == 0 ? (float)(-(cf.x + cf.y)) : (slot == 1 ? cx : cy);
     r.av = slot == 0 ? (float)(-(cf.z + cf.w)) : (slot == 1 ? cz : cw);
     r.area = (float)s.tri_area[t];
@@ -472,45 +480,99 @@ template <int G, int B, int MINB>
 __global__ void __launch_bounds__(B, MINB) k_sweep32(SweepView s, const uint32_t* order, uint32_t count) {
     extern __shared__ float stage_sm[];
     if (s.skip_at && *s.skip_at <= s.iteration) return;  // a refresh detection precedes this iteration
-    uint32_t t = blockIdx.x * B + threadIdx.x;
-    uint32_t gi = t / G;
-    if (gi >= count) return;  // whole groups leave together
-    uint32_t lane = threadIdx.x & (G - 1);
-    unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
-    solve_vertex32<G, B>(s, order[gi], lane, mask, stage_sm);
+    const uint32_t lane = threadIdx.x & (G - 1);
+    const unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
+    constexpr uint32_t kGroups = B / G;
+    // whole groups step together; a persistent grid loops over the colour
+    for (uint32_t gi = blockIdx.x * kGroups + threadIdx.x / G; gi < count; gi += gridDim.x * kGroups)
+        solve_vertex32<G, B>(s, order[gi], lane, mask, stage_sm);
 }
 
-template <int G, int MINB>
-void launch_g32(const SweepView& s, const uint32_t* order, uint32_t count, cudaStream_t st) {
-    constexpr int B = 128;
-    size_t smem = (size_t)Stage<G>::floats * B * sizeof(float);
-    allow_dynamic_smem(k_sweep32<G, B, MINB>, smem);
+template <int G, int B>
+constexpr size_t stage_bytes() {
+    return (size_t)Stage<G>::floats * B * sizeof(float);
+}
+
+template <int G, int B, int MINB>
+void launch_k32(const SweepView& s, const uint32_t* order, uint32_t count, cudaStream_t st, unsigned cap) {
+    constexpr size_t smem = stage_bytes<G, B>();
+    static std::atomic<uint64_t> raised{0};  // devices on which the limit is raised
+    allow_dynamic_smem_once(k_sweep32<G, B, MINB>, smem, raised);
     uint64_t threads = (uint64_t)count * G;
     unsigned grid = (unsigned)((threads + B - 1) / B);
+    if (cap && grid > cap) grid = cap;
     k_sweep32<G, B, MINB><<<grid, B, smem, st>>>(s, order, count);
 }
 
-template <int G>
-void launch_g32_cap(const SweepView& s, const uint32_t* order, uint32_t count, int minb, cudaStream_t st) {
-    if (minb >= 8) launch_g32<G, 8>(s, order, count, st);
-    else if (minb >= 6) launch_g32<G, 6>(s, order, count, st);
-    else if (minb == 5) launch_g32<G, 5>(s, order, count, st);
-    else if (minb == 4) launch_g32<G, 4>(s, order, count, st);
-    else launch_g32<G, 3>(s, order, count, st);
+template <int G, int B, int MINB>
+unsigned resident_k32() {
+    constexpr size_t smem = stage_bytes<G, B>();
+    allow_dynamic_smem(k_sweep32<G, B, MINB>, smem);
+    int dev = 0, sms = 0, per = 0;
+    CC_CUDA(cudaGetDevice(&dev));
+    CC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sweep32<G, B, MINB>, B, smem));
+    return (unsigned)(sms * (per > 0 ? per : 1));
 }
+
+// (lanes, cap, block) -> kernel instance; blocks of 64 and 256 threads exist
+// for 8 and 16 lanes at the register budgets of caps 3-4 (64) and 4, 6, 8 (256)
+template <int G, class F>
+auto dispatch_cap32(const SweepVariant& v, F&& f) {
+    if (v.block == 64) {
+        if (v.cap >= 4) return f.template operator()<G, 64, 8>();
+        return f.template operator()<G, 64, 6>();
+    }
+    if (v.block == 256) {
+        if (v.cap >= 8) return f.template operator()<G, 256, 4>();
+        if (v.cap >= 6) return f.template operator()<G, 256, 3>();
+        return f.template operator()<G, 256, 2>();
+    }
+    if (v.cap >= 8) return f.template operator()<G, 128, 8>();
+    if (v.cap >= 6) return f.template operator()<G, 128, 6>();
+    if (v.cap == 5) return f.template operator()<G, 128, 5>();
+    if (v.cap == 4) return f.template operator()<G, 128, 4>();
+    return f.template operator()<G, 128, 3>();
+}
+
+template <class F>
+auto dispatch32(const SweepVariant& v, F&& f) {
+    switch (v.lanes) {
+        case 4: return dispatch_cap32<4>(SweepVariant{4, v.cap, 128, v.persistent}, f);
+        case 16: return dispatch_cap32<16>(v, f);
+        case 32: return dispatch_cap32<32>(SweepVariant{32, v.cap, 128, v.persistent}, f);
+        default: return dispatch_cap32<8>(v, f);
+    }
+}
+
+struct Launch32 {
+    const SweepView& s;
+    const uint32_t* order;
+    uint32_t count;
+    cudaStream_t st;
+    unsigned cap;
+    template <int G, int B, int MINB>
+    int operator()() const {
+        launch_k32<G, B, MINB>(s, order, count, st, cap);
+        return 0;
+    }
+};
+struct Resident32 {
+    template <int G, int B, int MINB>
+    unsigned operator()() const {
+        return resident_k32<G, B, MINB>();
+    }
+};
 
 }  // namespace
 
-// variant = lanes per vertex (4, 8, 16 or 32) | occupancy cap (blocks per SM) << 8
-void launch_sweep32(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st) {
+void launch_sweep32(const SweepView& s, const uint32_t* order, uint32_t count, int variant, cudaStream_t st,
+                    unsigned grid_cap) {
     if (count == 0) return;
-    int lanes = variant & 0xff, minb = variant >> 8;
-    switch (lanes) {
-        case 4: launch_g32_cap<4>(s, order, count, minb, st); break;
-        case 16: launch_g32_cap<16>(s, order, count, minb, st); break;
-        case 32: launch_g32_cap<32>(s, order, count, minb, st); break;
-        default: launch_g32_cap<8>(s, order, count, minb, st); break;
-    }
+    SweepVariant v = decode_variant(variant);
+    dispatch32(v, Launch32{s, order, count, st, v.persistent ? grid_cap : 0u});
 }
+
+unsigned sweep32_resident_blocks(int variant) { return dispatch32(decode_variant(variant), Resident32{}); }
 
 }  // namespace cc

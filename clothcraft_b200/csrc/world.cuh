@@ -36,7 +36,7 @@ struct Lbvh {
     DBuf<unsigned long long> bounds;  // 6 order keys
     RadixSorter sorter;
     // returns the number of this library's kernels launched
-    int build(const Box* prim_box, const uint32_t* ids, uint32_t m, cudaStream_t s);
+    int build(const Box* prim_box, const uint32_t* ids, uint32_t m, cudaStream_t s, unsigned int* err);
     LbvhView view(const Box* prim_box) const {
         return {m, node_box.ptr, child.ptr, leaf_prim.ptr, prim_box, node_max.ptr};
     }

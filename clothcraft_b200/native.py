@@ -36,6 +36,7 @@ SIGNATURES = {
     "cc_solver_world": (C.c_void_p, [C.c_void_p]),
     "cc_solver_stream": (C.c_void_p, [C.c_void_p]),
     "cc_solver_set_profiling": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "cc_solver_set_graphs": (C.c_int32, [C.c_void_p, C.c_int32]),
     "cc_solver_set_lanes": (C.c_int32, [C.c_void_p, C.c_int32]),
     "cc_solver_get_lanes": (C.c_int32, [C.c_void_p]),
     "cc_solver_set_lanes32": (C.c_int32, [C.c_void_p, C.c_int32]),

@@ -34,6 +34,7 @@ def main(argv=None):
     ap.add_argument("--precision", type=int, default=0, help="sweep arithmetic: 0 FP64, 1 FP32 assembly")
     ap.add_argument("--lanes32", type=int, default=8 | 4 << 8)
     ap.add_argument("--profile", action="store_true", help="time each iteration's sweeps with CUDA events")
+    ap.add_argument("--graphs", action="store_true", help="launch the iteration chunks as CUDA graphs")
     args = ap.parse_args(argv)
     sc = scenes.config1()
     z = np.load(FOLD_STATE)
@@ -52,6 +53,7 @@ def main(argv=None):
         s.init_mode = 1
     g.set_state(z["x"].astype(np.float64), z["v"].astype(np.float64), float(z["time"]))
     g.set_profiling(args.profile)
+    g.set_graphs(args.graphs)
     for k in range(args.steps):
         m = g.step_resident(s.to_c())
         print("step %d: %d iterations, %.2f ms, residual %s, sweeps %.3f ms in %d launches, detection %.3f ms "

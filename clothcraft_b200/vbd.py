@@ -291,6 +291,12 @@ class VbdSolver:
         native.load().cc_solver_set_profiling(self.h, 1 if enable else 0)
         return self
 
+    def set_graphs(self, enable: bool):
+        """Launch each step's iteration chunks as CUDA graphs (bitwise the
+        results of direct launches)."""
+        native.load().cc_solver_set_graphs(self.h, 1 if enable else 0)
+        return self
+
     def set_lanes32(self, lanes: int):
         """Threads per vertex solve of the FP32-assembly sweep (4, 8, 16 or 32,
         optionally | cap << 8), or 0 to autotune on the next FP32 step."""

@@ -291,6 +291,16 @@ uint64_t cc_solver_total(const cc_solver* solver);
  * (the wgpu backend times its compute pass with timestamp queries,
  * src/gpu_vbd/cache.rs:16-33). */
 void* cc_solver_stream(const cc_solver* solver);
+/* When enabled, each chunk of iterations the step enqueues ahead of the
+ * device (all iterations without a residual target; max(check_every, 4)
+ * with one) is captured into a CUDA graph and launched as one; the
+ * executable graph is updated in place while the chunk's topology stays the
+ * same (colour count, placement of the residual checks) and instantiated
+ * again when it changes, e.g. after a colouring with another colour count.
+ * Results are bitwise those of direct launches. Off by default; ignored
+ * while profiling is on. No reference counterpart (the wgpu backend records
+ * one dispatch per colour per iteration, src/gpu_vbd.rs:398-404). */
+int32_t cc_solver_set_graphs(cc_solver* solver, int32_t enable);
 /* When enabled, each iteration's colour sweeps (launched back to back) are
  * bracketed by one pair of CUDA events and cc_metrics.sweep_ms reports their
  * summed device time over the iterations the step ran. */
@@ -298,7 +308,10 @@ int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
 /* Threads that cooperate on one vertex's local solve (1, 2, 4, 8, 16 or 32),
  * optionally | (cap << 8) with cap = 3, 4, 5, 6 or 8 resident 128-thread
  * blocks per SM (a register budget; default 3; above 3 registers spill to
- * local memory); 0 (the default) lets the solver time the
+ * local memory), | (1 << 16) for a persistent grid (at most the resident
+ * blocks, each looping over the colour's vertices), | (1 << 17) or (2 << 17)
+ * for blocks of 64 or 256 threads (4 or 8 lanes; caps 3-4 or 4, 6, 8) at the
+ * same register budget; 0 (the default) lets the solver time the
  * candidates on its first step and keep the fastest. get_lanes returns the
  * same encoding. Two solvers take bitwise-identical steps only with the same
  * setting. No reference counterpart (the wgpu backend always uses a 32-lane
@@ -306,8 +319,9 @@ int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
 int32_t cc_solver_set_lanes(cc_solver* solver, int32_t lanes);
 int32_t cc_solver_get_lanes(const cc_solver* solver);
 /* The same for the CC_SWEEP_FP32 sweep: lanes 4, 8, 16 or 32, optionally
- * | (cap << 8) with cap = 3, 4, 5, 6 or 8; 0 (the default) autotunes on the
- * first FP32 step. */
+ * | (cap << 8) with cap = 3, 4, 5, 6 or 8, the persistent bit and the block
+ * size (64 or 256 threads for 8 or 16 lanes); 0 (the default) autotunes on
+ * the first FP32 step. */
 int32_t cc_solver_set_lanes32(cc_solver* solver, int32_t lanes);
 int32_t cc_solver_get_lanes32(const cc_solver* solver);
 

@@ -105,7 +105,10 @@ def test_fp32_fold_fixed_iterations_within_1e5_m_of_oracle():
     xo, _, _, mo = oracle.Solver(sc, threads=THREADS).step(x, v, t, st)
     err = float(np.linalg.norm(xg - xo, axis=1).max())
     assert err <= POSITION_TOL_M, err
-    assert mg["detection_updates"] == mo["detection_updates"] and mg["contact_terms"] == mo["contact_terms"]
+    # refresh detections run at iterates ~1e-7 m apart, so terms right at the
+    # query radius may differ by a few; the detection count may not
+    assert mg["detection_updates"] == mo["detection_updates"]
+    assert abs(mg["contact_terms"] - mo["contact_terms"]) <= 1e-3 * mo["contact_terms"]
 
 
 def test_fp32_fold_reaches_the_residual_target_like_fp64():

@@ -316,3 +316,74 @@ def test_step_into_pinned_arrays_equals_step():
     assert np.array_equal(xh, before[0]) and np.array_equal(vh, before[1])
     with pytest.raises(ValueError):
         b.step_into(xh[:, :2], vh, tb, st)
+
+
+PERSISTENT, B64, B256 = 1 << 16, 1 << 17, 2 << 17
+
+
+@pytest.mark.parametrize("fp32,lanes", [(False, 4), (False, 8), (True, 8), (True, 16)])
+def test_persistent_grids_and_block_sizes_give_identical_steps(fp32, lanes):
+    """A persistent grid (each block looping over the colour's vertices) and
+    blocks of 64 or 256 threads change only the schedule: on the fold state,
+    where a colour has ~16k vertices and the persistent grid loops, every
+    variant gives the bits of the 128-thread one-pass grid."""
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sheet256_fold_state.npz"))
+    x, v, t = z["x"].astype(np.float64), z["v"].astype(np.float64), float(z["time"])
+    sc = scenes.config1()
+    s = sc.settings
+    s.iterations = 6
+    s.sweep_precision = 1 if fp32 else 0
+    st = s.to_c()
+
+    def run(variant):
+        g = VbdSolver(sc)
+        (g.set_lanes32 if fp32 else g.set_lanes)(variant)
+        g.set_state(x, v, t)
+        for _ in range(2):
+            g.step_resident(st)
+        return g.get_state()
+
+    xr, vr, _ = run(lanes | 4 << 8)
+    for extra in (PERSISTENT, B64, B256, B64 | PERSISTENT):
+        xs, vs, _ = run(lanes | 4 << 8 | extra)
+        assert np.array_equal(xs, xr) and np.array_equal(vs, vr), extra
+
+
+def test_invalid_block_variants_are_rejected():
+    s = VbdSolver(contact_scene(8, seed=1))
+    for bad in (16 | 4 << 8 | B64, 2 | 4 << 8 | B256, 8 | 5 << 8 | B64, 8 | 4 << 8 | 3 << 17, 8 | 4 << 8 | 1 << 19):
+        with pytest.raises(VbdError):
+            s.set_lanes(bad)
+    for bad in (4 | 4 << 8 | B64, 32 | 4 << 8 | B256):
+        with pytest.raises(VbdError):
+            s.set_lanes32(bad)
+
+
+@pytest.mark.parametrize("target", [False, True])
+def test_graph_launches_give_the_bits_of_direct_launches(target):
+    """CUDA-graph chunks (captured, updated in place or re-instantiated when
+    a colouring changes the topology) against direct launches on the fold
+    state: fixed iterations, and the residual target with acceleration,
+    stall refreshes and the chunked look-ahead."""
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sheet256_fold_state.npz"))
+    x, v, t = z["x"].astype(np.float64), z["v"].astype(np.float64), float(z["time"])
+    sc = scenes.config1()
+    s = sc.settings
+    if target:
+        s.iterations, s.residual_tolerance, s.residual_check_every, s.stall_refresh = 200, 1e-3, 2, 2
+        s.acceleration = 0.95
+    st = s.to_c()
+    out = []
+    for graphs in (False, True):
+        g = VbdSolver(sc).set_lanes(8 | 4 << 8).set_graphs(graphs)
+        g.set_state(x, v, t)
+        its = [g.step_resident(st)["iterations"] for _ in range(3)]
+        out.append((g.get_state(), its))
+    (xa, va, _), ia = out[0]
+    (xb, vb, _), ib = out[1]
+    assert ia == ib
+    assert np.array_equal(xa, xb) and np.array_equal(va, vb)
