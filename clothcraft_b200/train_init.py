@@ -71,7 +71,7 @@ def _drive(sc, solver):
 
 
 def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, cap: int = 200, check: int = 2,
-             log=print, driven: bool = False):
+             log=print, driven: bool = False, acceleration: float = 0.0):
     """Plain vs learned init at a residual target on each scene: `warm` plain
     steps, then `steps` steps per init from the same state. Returns a list of
     per-scene dicts (mean iterations, device ms per step, learned-used fraction)."""
@@ -91,6 +91,7 @@ def evaluate(net, scene_list, warm: int, steps: int, tolerance: float = 1e-3, ca
                 h.set_mlp(net, 1)
             h.set_state(*start)
             st = sample_settings(sc, tolerance, cap, check, mode)
+            st.acceleration = acceleration
             its, ms, used = [], [], []
             for _ in range(steps):
                 if driven:
@@ -178,6 +179,7 @@ def main(argv=None):
     ap.add_argument("--evaluate", type=int, default=0, help="held-out seeds to evaluate on after training")
     ap.add_argument("--eval-steps", type=int, default=30)
     ap.add_argument("--weights", default=None, help="skip training: evaluate these weights")
+    ap.add_argument("--acceleration", type=float, default=0.0, help="Chebyshev rho of the evaluation steps")
     args = ap.parse_args(argv)
     out = args.out or os.path.join(DATA, "%s_init_mlp.npz" % args.kind)
     if args.weights:
@@ -210,7 +212,8 @@ def main(argv=None):
             held = crumple_scenes(args.evaluate, first_seed=20000, workers=args.workers)
             warm = 30
         print("evaluating on %d held-out seeds (tolerance 1e-3)" % len(held), flush=True)
-        rows = evaluate(net, held, warm, args.eval_steps, driven=args.kind == "crumple")
+        rows = evaluate(net, held, warm, args.eval_steps, driven=args.kind == "crumple",
+                        acceleration=args.acceleration)
         tr = [r["time_ratio"] for r in rows]
         ir = [r["iteration_ratio"] for r in rows]
         print("held-out summary: time ratio plain/learned mean %.3f median %.3f; iteration ratio mean %.3f median %.3f"
