@@ -426,10 +426,14 @@ def main():
     L.cc_solver_set_profiling(learned.h, 0)
     # ---- plain adaptive init at equal residual
     t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
-    # ---- the value leg's settings with each iteration chunk launched as a CUDA graph
-    graph_solver = make(1)
-    graph_solver.set_graphs(True)
-    t_g, mets_g = leg(graph_solver, lambda: graph_solver.step_resident(st_l), K)
+    # ---- the value leg's settings with every kernel launched directly (no CUDA
+    # graphs) and without the per-iteration sweep events
+    direct_solver = make(1)
+    direct_solver.set_graphs(False)
+    t_g, mets_g = leg(direct_solver, lambda: direct_solver.step_resident(st_l), K)
+    # ---- the value leg's settings, CUDA graphs, without the sweep events
+    quiet_solver = make(1)
+    t_q, mets_q = leg(quiet_solver, lambda: quiet_solver.step_resident(st_l), K)
     # ---- both inits at the other sweep precision (same target and acceleration)
     other = 1 - SWEEP_PRECISION
     other_legs = {}
@@ -555,9 +559,13 @@ def main():
         "learned_vs_plain_time_ratio": t_p / t_l,
         "learned_init_used_fraction": float(np.mean([m["init_used"] for m in mets_l])),
         "acceleration": ACCELERATION,
-        "graphs": dict(summary(t_g, mets_g), note="the learned leg with every iteration chunk captured into a "
-                                                   "CUDA graph and launched as one (updated in place while its "
-                                                   "topology holds)"),
+        "launch_forms": {
+            "graphs_with_sweep_events": {"steps_per_s": world * K / (t_l / 1000.0), "ms_per_step": t_l / K},
+            "graphs": {"steps_per_s": world * K / (t_q / 1000.0), "ms_per_step": t_q / K},
+            "direct_launches": {"steps_per_s": world * K / (t_g / 1000.0), "ms_per_step": t_g / K},
+            "note": "the value leg (iteration chunks launched as CUDA graphs, per-iteration sweep events "
+                    "recorded by event nodes) against the same steps without the events, and with every "
+                    "kernel launched directly; identical iterates"},
         "sweep_precision": ("fp32 element assembly" if SWEEP_PRECISION else "fp64"),
         "other_precision": {"sweep_precision": ("fp32 element assembly" if other else "fp64"),
                             "learned": summary(*other_legs[1]), "plain": summary(*other_legs[0]),

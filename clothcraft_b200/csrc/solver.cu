@@ -589,9 +589,15 @@ struct cc_solver {
     }
 
     // CUDA-graph launch of the iteration chunks (cc_solver_set_graphs)
-    bool graphs = false;
+    bool graphs = true;
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_instantiations = 0, graph_updates = 0;
+    // an event record that also times inside a captured graph (an external
+    // event node records the event each time the graph runs)
+    void record_event(cudaEvent_t e, bool captured) {
+        if (captured) CC_CUDA(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
+        else CC_CUDA(cudaEventRecord(e, stream));
+    }
     void launch_captured_chunk() {
         cudaGraph_t g = nullptr;
         CC_CUDA(cudaStreamEndCapture(stream, &g));
@@ -919,7 +925,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         // executable graph is updated in place while the chunk's topology (the
         // colour count and the placement of the residual checks) stays the
         // same, and instantiated anew when it changes
-        const bool capture = graphs && !profiling;
+        const bool capture = graphs;
         for (uint32_t c0 = it0; c0 < s.iterations; c0 += chunk) {
             uint32_t c1 = std::min(s.iterations, c0 + chunk);
             if (capture) CC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
@@ -935,7 +941,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                         CC_CUDA(cudaEventCreate(&e));
                         prof_events.push_back(e);
                     }
-                    CC_CUDA(cudaEventRecord(prof_events[prof_used], stream));
+                    record_event(prof_events[prof_used], capture);
                 }
                 for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
                     uint32_t cnt = off[c + 1] - off[c];
@@ -944,7 +950,7 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                     ++own_launches;
                 }
                 if (profiling) {
-                    CC_CUDA(cudaEventRecord(prof_events[prof_used + 1], stream));
+                    record_event(prof_events[prof_used + 1], capture);
                     prof_pairs.push_back({prof_used, it});
                     prof_used += 2;
                 }

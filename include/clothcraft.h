@@ -297,9 +297,11 @@ void* cc_solver_stream(const cc_solver* solver);
  * executable graph is updated in place while the chunk's topology stays the
  * same (colour count, placement of the residual checks) and instantiated
  * again when it changes, e.g. after a colouring with another colour count.
- * Results are bitwise those of direct launches. Off by default; ignored
- * while profiling is on. No reference counterpart (the wgpu backend records
- * one dispatch per colour per iteration, src/gpu_vbd.rs:398-404). */
+ * Results are bitwise those of direct launches. On by default (0 launches
+ * every kernel directly). With profiling on, the sweep timings are recorded
+ * by event nodes inside the graphs. No reference counterpart (the wgpu
+ * backend records one dispatch per colour per iteration,
+ * src/gpu_vbd.rs:398-404). */
 int32_t cc_solver_set_graphs(cc_solver* solver, int32_t enable);
 /* When enabled, each iteration's colour sweeps (launched back to back) are
  * bracketed by one pair of CUDA events and cc_metrics.sweep_ms reports their
