@@ -16,7 +16,11 @@
 #include <mutex>
 #include <set>
 
+#include <cooperative_groups.h>
+
 #include "world.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace cc {
 
@@ -497,6 +501,17 @@ __global__ void k_cover_and_scale(WorldView w, const double4* centers, int have_
 }
 
 // ------------------------------------------------------------ pair queries
+// Warp-aggregated append: the lanes that reach this call together take
+// consecutive slots of an output list with one atomic per warp instead of
+// one per lane (the candidate and raw-contact lists are order-free: pairs are
+// consumed as a set, contacts are sorted canonically afterwards).
+__device__ __forceinline__ unsigned long long append_slot(unsigned long long* count) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (g.thread_rank() == 0) base = atomicAdd(count, (unsigned long long)g.size());
+    return g.shfl(base, 0) + g.thread_rank();
+}
+
 // VF candidates (candidates.rs:29-37): every point against triangles, pairs
 // with box distance <= search, not both fixed, triangle not adjacent.
 __global__ void k_vf_query(WorldView w, LbvhView tri_moving, LbvhView tri_fixed, double search2, uint2* out,
@@ -509,7 +524,7 @@ __global__ void k_vf_query(WorldView w, LbvhView tri_moving, LbvhView tri_fixed,
         auto visit = [&](uint32_t t) {
             uint3 ids = w.tri[t];
             if (adjacent(w, v, ids.x) || adjacent(w, v, ids.y) || adjacent(w, v, ids.z)) return;
-            unsigned long long k = atomicAdd(count, 1ull);
+            unsigned long long k = append_slot(count);
             if (k < cap) out[k] = make_uint2(v, t);
         };
         bool ok = lbvh_traverse(tri_moving, node_ok, leaf_ok, visit);
@@ -537,12 +552,12 @@ __global__ void k_ee_query(WorldView w, const uint32_t* edge_moving, uint32_t n_
         };
         auto visit_moving = [&](uint32_t f) {
             if (f <= e || filtered(f)) return;
-            unsigned long long i = atomicAdd(count, 1ull);
+            unsigned long long i = append_slot(count);
             if (i < cap) out[i] = make_uint2(e, f);
         };
         auto visit_fixed = [&](uint32_t f) {
             if (filtered(f)) return;
-            unsigned long long i = atomicAdd(count, 1ull);
+            unsigned long long i = append_slot(count);
             if (i < cap) out[i] = make_uint2(e, f);
         };
         bool ok = lbvh_traverse_above(edge_moving_t, e, node_ok, leaf_ok, visit_moving);
@@ -581,7 +596,7 @@ __device__ __forceinline__ void push_contact(unsigned kind, uint32_t i0, uint32_
             sw(1, 3);
         }
     }
-    unsigned long long k = atomicAdd(count, 1ull);
+    unsigned long long k = append_slot(count);
     if (k < cap) {
         hi[k] = ((unsigned long long)kind << (2 * nb)) | ((unsigned long long)v[0] << nb) | (unsigned long long)v[1];
         lo[k] = ((unsigned long long)v[2] << nb) | (unsigned long long)v[3];
@@ -604,27 +619,51 @@ struct NarrowOut {
     uint32_t nb;  // bits per vertex id in the contact keys
 };
 
-__global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
-                         unsigned long long n_ee, double query_radius, const unsigned long long* max_abs_bits,
-                         int prune, NarrowOut o) {
+// The narrow phase runs in two passes so that the FP64 closest-feature work
+// fills whole warps: the prune pass drops the pairs whose boxes are farther
+// apart than the padded query radius (world.rs:431-438, 482-486) and appends
+// the survivors' pair indices (VF first, then EE offset by n_vf) to `surv`;
+// the evaluation pass walks the survivors. Without pruning every pair survives.
+__global__ void k_narrow_prune(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
+                               unsigned long long n_ee, double query_radius, const unsigned long long* max_abs_bits,
+                               int prune, uint32_t* surv, unsigned long long* n_surv,
+                               unsigned long long* rejections) {
     double scale = fmax(query_radius, bitsd(*max_abs_bits));
     double pr = query_radius + 64.0 * 2.220446049250313e-16 * scale;
     double padded2 = pr * pr;
-    unsigned long long nvf = 0, nee = 0, nrej = 0;
+    unsigned long long nrej = 0;
     unsigned long long total = n_vf + n_ee;
     for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
          k += (unsigned long long)gridDim.x * blockDim.x) {
+        bool keep = true;
+        if (prune) {
+            if (k < n_vf) {
+                Box pb;
+                box_of1(ld3(w.x, vf[k].x), pb);
+                keep = !(box_dist2(pb, w.tri_box[vf[k].y]) > padded2);
+            } else {
+                uint2 p = ee[k - n_vf];
+                keep = !(box_dist2(w.edge_box[p.x], w.edge_box[p.y]) > padded2);
+            }
+        }
+        if (keep) surv[append_slot(n_surv)] = (uint32_t)k;
+        else ++nrej;
+    }
+    for (int s = 16; s > 0; s >>= 1) nrej += __shfl_xor_sync(0xffffffffu, nrej, s);
+    if ((threadIdx.x & 31) == 0 && nrej) atomicAdd(rejections, nrej);
+}
+
+__global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
+                         const uint32_t* surv, const unsigned long long* n_surv, double query_radius,
+                         NarrowOut o) {
+    unsigned long long nvf = 0, nee = 0, nrej = 0;
+    const unsigned long long total = *n_surv;
+    for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < total;
+         s += (unsigned long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = surv[s];
         if (k < n_vf) {
             uint32_t v = vf[k].x, t = vf[k].y;
             d3 xv = ld3(w.x, v);
-            if (prune) {
-                Box pb;
-                box_of1(xv, pb);
-                if (box_dist2(pb, w.tri_box[t]) > padded2) {
-                    ++nrej;
-                    continue;
-                }
-            }
             uint3 ids = w.tri[t];
             int kind;
             uint32_t fid;
@@ -651,10 +690,6 @@ __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, 
         } else {
             unsigned long long kk = k - n_vf;
             uint32_t e = ee[kk].x, f = ee[kk].y;
-            if (prune && box_dist2(w.edge_box[e], w.edge_box[f]) > padded2) {
-                ++nrej;
-                continue;
-            }
             uint2 ids = w.edges[e], js = w.edges[f];
             d3 a = ld3(w.x, ids.x), b = ld3(w.x, ids.y), c = ld3(w.x, js.x), dd = ld3(w.x, js.y);
             double s, t;
@@ -1164,9 +1199,17 @@ void World::detect(double query_radius, double radius, double relaxation, double
         NarrowOut o{raw_hi_.ptr,   raw_lo_.ptr,    raw_eps_.ptr,   raw_idx_.ptr,      raw_cap_, &sd->n_raw,
                     dist_bits_.ptr, &sd->vf_count, &sd->ee_count, &sd->rejections, nb};
         unsigned long long total = n_vf + n_ee;
-        k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee, query_radius,
-                                                                    &sd->max_abs_bits, prune ? 1 : 0, o);
-        launches_ += 2;
+        if (total > 0xffffffffull) throw Failure{CC_ERR_CAPACITY, "OGC candidate pairs exceed 2^32"};
+        surv_.reserve(std::max<size_t>((size_t)total, 1));
+        CC_CUDA(cudaMemsetAsync(&sd->n_surv, 0, sizeof(unsigned long long), stream_));
+        CC_CUDA(cudaMemsetAsync(&sd->rejections, 0, sizeof(unsigned long long), stream_));
+        k_narrow_prune<<<grid_for((size_t)total, 256), 256, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee,
+                                                                          query_radius, &sd->max_abs_bits,
+                                                                          prune ? 1 : 0, surv_.ptr, &sd->n_surv,
+                                                                          &sd->rejections);
+        k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, surv_.ptr,
+                                                                    &sd->n_surv, query_radius, o);
+        launches_ += 3;
         CC_CUDA(cudaGetLastError());
         mark(3);
         sync_stats();
