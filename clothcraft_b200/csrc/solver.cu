@@ -91,6 +91,7 @@ struct StepScalars {
     double e_cand, best_e;  // learned-guess scale search
     unsigned int clipped_best;
     int take;
+    unsigned long long p95_bits, ext_max_bits;  // extension metric keys of the step's end
 };
 
 __global__ void k_step_begin(uint32_t n, const double4* x0, const double4* v0, const double4* px, const double4* pv,
@@ -363,11 +364,14 @@ __global__ void k_stretch(uint32_t nt, const int4* tv, const double4* coef, cons
     }
 }
 
-__global__ void k_p95(uint32_t nt, const unsigned long long* key_sorted, const double* cum, double total,
-                      unsigned long long* out_bits) {
+// extension P95 (the first sorted key whose cumulative area reaches 95 % of the
+// total) and maximum, into the step scalars (read with the step's last sync)
+__global__ void k_p95(uint32_t nt, const unsigned long long* key_sorted, const double* cum, StepScalars* sc) {
+    const double total = cum[nt - 1];
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
         bool hit = cum[t] >= 0.95 * total && (t == 0 || !(cum[t - 1] >= 0.95 * total));
-        if (hit) *out_bits = key_sorted[t];
+        if (hit) sc->p95_bits = key_sorted[t];
+        if (t == nt - 1) sc->ext_max_bits = key_sorted[t];
     }
 }
 
@@ -455,7 +459,7 @@ struct cc_solver {
     double pred_time = 0.0, pred_damping = 0.0;
     double pred_g[3] = {0, 0, 0};
     // metrics scratch
-    DBuf<unsigned long long> ext_key, ext_key_s, p95_bits;
+    DBuf<unsigned long long> ext_key, ext_key_s;
     DBuf<double> ext_w, ext_w_s, ext_cum;
     RadixSorter ext_sorter;
     DBuf<double> ext_scan;
@@ -1064,20 +1068,14 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         own_launches += ext_sorter.sort_pairs(ext_key.ptr, ext_key_s.ptr, ext_w.ptr, ext_w_s.ptr, n_tri, 64, stream,
                                               &sc.ptr->error, DERR_SORT_WAIT);
         own_launches += inclusive_sum(ext_w_s.ptr, ext_cum.ptr, n_tri, ext_scan, stream);
-        double total = 0.0;
-        unsigned long long kmax = 0, kp = order_key(0.0);
-        CC_CUDA(cudaMemcpyAsync(&total, ext_cum.ptr + n_tri - 1, 8, cudaMemcpyDeviceToHost, stream));
-        CC_CUDA(cudaMemcpyAsync(&kmax, ext_key_s.ptr + n_tri - 1, 8, cudaMemcpyDeviceToHost, stream));
-        CC_CUDA(cudaStreamSynchronize(stream));
-        CC_CUDA(cudaMemcpyAsync(p95_bits.ptr, &kp, 8, cudaMemcpyHostToDevice, stream));
-        k_p95<<<grid_for(n_tri, 256), 256, 0, stream>>>(n_tri, ext_key_s.ptr, ext_cum.ptr, total, p95_bits.ptr);
-        CC_CUDA(cudaMemcpyAsync(&kp, p95_bits.ptr, 8, cudaMemcpyDeviceToHost, stream));
-        CC_CUDA(cudaStreamSynchronize(stream));
-        p95 = from_order_key(kp);
-        emax = from_order_key(kmax);
+        k_p95<<<grid_for(n_tri, 256), 256, 0, stream>>>(n_tri, ext_key_s.ptr, ext_cum.ptr, sc.ptr);
     }
     CC_CUDA(cudaEventRecord(ev1, stream));
     read_scalars();
+    if (n_tri) {
+        p95 = from_order_key(sc_h.ptr->p95_bits);
+        emax = from_order_key(sc_h.ptr->ext_max_bits);
+    }
     const bool metric_sort_failed = (sc_h.ptr->error & DERR_SORT_WAIT) != 0;  // the step is committed already
     float gms = 0.f;
     CC_CUDA(cudaEventElapsedTime(&gms, ev0, ev1));
@@ -1380,7 +1378,6 @@ int32_t cc_solver_create(const cc_mesh* mesh, const cc_surface* obstacle, const 
         h->ext_w.reserve(T);
         h->ext_w_s.reserve(T);
         h->ext_cum.reserve(T);
-        h->p95_bits.reserve(1);
         h->residual.zero(n, st);
         h->coloring.init((uint32_t)n, st);
         // initial state
