@@ -619,51 +619,27 @@ struct NarrowOut {
     uint32_t nb;  // bits per vertex id in the contact keys
 };
 
-// The narrow phase runs in two passes so that the FP64 closest-feature work
-// fills whole warps: the prune pass drops the pairs whose boxes are farther
-// apart than the padded query radius (world.rs:431-438, 482-486) and appends
-// the survivors' pair indices (VF first, then EE offset by n_vf) to `surv`;
-// the evaluation pass walks the survivors. Without pruning every pair survives.
-__global__ void k_narrow_prune(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
-                               unsigned long long n_ee, double query_radius, const unsigned long long* max_abs_bits,
-                               int prune, uint32_t* surv, unsigned long long* n_surv,
-                               unsigned long long* rejections) {
+__global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
+                         unsigned long long n_ee, double query_radius, const unsigned long long* max_abs_bits,
+                         int prune, NarrowOut o) {
     double scale = fmax(query_radius, bitsd(*max_abs_bits));
     double pr = query_radius + 64.0 * 2.220446049250313e-16 * scale;
     double padded2 = pr * pr;
-    unsigned long long nrej = 0;
+    unsigned long long nvf = 0, nee = 0, nrej = 0;
     unsigned long long total = n_vf + n_ee;
     for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < total;
          k += (unsigned long long)gridDim.x * blockDim.x) {
-        bool keep = true;
-        if (prune) {
-            if (k < n_vf) {
-                Box pb;
-                box_of1(ld3(w.x, vf[k].x), pb);
-                keep = !(box_dist2(pb, w.tri_box[vf[k].y]) > padded2);
-            } else {
-                uint2 p = ee[k - n_vf];
-                keep = !(box_dist2(w.edge_box[p.x], w.edge_box[p.y]) > padded2);
-            }
-        }
-        if (keep) surv[append_slot(n_surv)] = (uint32_t)k;
-        else ++nrej;
-    }
-    for (int s = 16; s > 0; s >>= 1) nrej += __shfl_xor_sync(0xffffffffu, nrej, s);
-    if ((threadIdx.x & 31) == 0 && nrej) atomicAdd(rejections, nrej);
-}
-
-__global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
-                         const uint32_t* surv, const unsigned long long* n_surv, double query_radius,
-                         NarrowOut o) {
-    unsigned long long nvf = 0, nee = 0, nrej = 0;
-    const unsigned long long total = *n_surv;
-    for (unsigned long long s = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; s < total;
-         s += (unsigned long long)gridDim.x * blockDim.x) {
-        const unsigned long long k = surv[s];
         if (k < n_vf) {
             uint32_t v = vf[k].x, t = vf[k].y;
             d3 xv = ld3(w.x, v);
+            if (prune) {
+                Box pb;
+                box_of1(xv, pb);
+                if (box_dist2(pb, w.tri_box[t]) > padded2) {
+                    ++nrej;
+                    continue;
+                }
+            }
             uint3 ids = w.tri[t];
             int kind;
             uint32_t fid;
@@ -690,6 +666,10 @@ __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, 
         } else {
             unsigned long long kk = k - n_vf;
             uint32_t e = ee[kk].x, f = ee[kk].y;
+            if (prune && box_dist2(w.edge_box[e], w.edge_box[f]) > padded2) {
+                ++nrej;
+                continue;
+            }
             uint2 ids = w.edges[e], js = w.edges[f];
             d3 a = ld3(w.x, ids.x), b = ld3(w.x, ids.y), c = ld3(w.x, js.x), dd = ld3(w.x, js.y);
             double s, t;
@@ -1199,17 +1179,9 @@ void World::detect(double query_radius, double radius, double relaxation, double
         NarrowOut o{raw_hi_.ptr,   raw_lo_.ptr,    raw_eps_.ptr,   raw_idx_.ptr,      raw_cap_, &sd->n_raw,
                     dist_bits_.ptr, &sd->vf_count, &sd->ee_count, &sd->rejections, nb};
         unsigned long long total = n_vf + n_ee;
-        if (total > 0xffffffffull) throw Failure{CC_ERR_CAPACITY, "OGC candidate pairs exceed 2^32"};
-        surv_.reserve(std::max<size_t>((size_t)total, 1));
-        CC_CUDA(cudaMemsetAsync(&sd->n_surv, 0, sizeof(unsigned long long), stream_));
-        CC_CUDA(cudaMemsetAsync(&sd->rejections, 0, sizeof(unsigned long long), stream_));
-        k_narrow_prune<<<grid_for((size_t)total, 256), 256, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee,
-                                                                          query_radius, &sd->max_abs_bits,
-                                                                          prune ? 1 : 0, surv_.ptr, &sd->n_surv,
-                                                                          &sd->rejections);
-        k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, surv_.ptr,
-                                                                    &sd->n_surv, query_radius, o);
-        launches_ += 3;
+        k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee, query_radius,
+                                                                    &sd->max_abs_bits, prune ? 1 : 0, o);
+        launches_ += 2;
         CC_CUDA(cudaGetLastError());
         mark(3);
         sync_stats();

@@ -80,7 +80,6 @@ struct DetectStats {  // read back after each detection
     unsigned long long max_move_bits;          // max |x - cache centre|^2 (moving)
     unsigned long long max_abs_bits;           // max |x| component (all)
     unsigned long long intersect_key;          // validate_start: first (i<<32|j)
-    unsigned long long n_surv;                 // narrow-phase pairs that pass the box prune
     unsigned int error;
     unsigned int rebuild;
 };
@@ -160,7 +159,6 @@ class World {
     double cache_R_ = 0, cache_skin_ = 0;
     DBuf<double4> cache_centers_;
     DBuf<uint2> vf_, ee_;
-    DBuf<uint32_t> surv_;  // narrow-phase survivors of the box prune
     size_t vf_cap_ = 0, ee_cap_ = 0;
 
     // narrow phase + canonical set
