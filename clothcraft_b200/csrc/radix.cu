@@ -8,8 +8,8 @@ namespace cc {
 namespace {
 
 constexpr int kBlock = 256;              // threads per tile
-constexpr int kItems = 8;                // keys per thread
-constexpr int kTile = kBlock * kItems;   // 2048 keys per tile
+constexpr int kItems = 4;                // keys per thread
+constexpr int kTile = kBlock * kItems;   // 1024 keys per tile
 constexpr int kRadix = 256;              // 8-bit digits
 constexpr int kScanBlock = 1024;
 

@@ -2,7 +2,7 @@
 // (key, value) pairs with 8-bit digits, and exclusive / inclusive prefix sums.
 //
 // The sort reads every key once for the digit histograms of all its passes,
-// then runs one kernel per pass: each block takes the next tile of 2048 keys
+// then runs one kernel per pass: each block takes the next tile of 1024 keys
 // (tiles numbered in the order blocks start), ranks them stably among the
 // tile's keys of the same digit (warp match in index order, per-warp digit
 // counts across warps), publishes the tile's digit counts and adds its
