@@ -67,18 +67,6 @@ __device__ __forceinline__ Box box_union(const Box& a, const Box& b) {
     }
     return r;
 }
-__device__ __forceinline__ Box ldcg_box(const Box* p) {
-    Box b;
-    const double* s = reinterpret_cast<const double*>(p);
-    b.lo[0] = __ldcg(s + 0);
-    b.lo[1] = __ldcg(s + 1);
-    b.lo[2] = __ldcg(s + 2);
-    b.hi[0] = __ldcg(s + 3);
-    b.hi[1] = __ldcg(s + 4);
-    b.hi[2] = __ldcg(s + 5);
-    return b;
-}
-
 // ------------------------------------------------------------------- LBVH
 __global__ void k_bounds_init(unsigned long long* b) {
     if (threadIdx.x < 3) b[threadIdx.x] = ~0ull;
@@ -119,25 +107,70 @@ __device__ __forceinline__ unsigned long long spread21(unsigned long long v) {
     return v;
 }
 
-__global__ void k_morton(const Box* box, const uint32_t* ids, uint32_t m, const unsigned long long* b,
-                         unsigned long long* code, uint32_t* vals) {
-    double lo[3], ext[3];
+// 63-bit Morton code of a point in the centroid bounds, every axis scaled by
+// the largest extent (a cube), so that a nearly flat set keeps its flat
+// order: its thin axis then only reaches the low bits instead of being
+// stretched over all 21.
+__device__ __forceinline__ unsigned long long morton63(const double* c, const unsigned long long* b) {
+    double lo[3], ext = 0.0;
     for (int k = 0; k < 3; ++k) {
         lo[k] = from_order_key(b[k]);
-        ext[k] = from_order_key(b[3 + k]) - lo[k];
+        ext = fmax(ext, from_order_key(b[3 + k]) - lo[k]);
     }
+    unsigned long long code = 0;
+    for (int k = 0; k < 3; ++k) {
+        double t = ext > 0.0 ? (c[k] - lo[k]) / ext : 0.0;
+        double s = t * 2097152.0;
+        unsigned long long u = s <= 0.0 ? 0ull : (s >= 2097151.0 ? 2097151ull : (unsigned long long)s);
+        code |= spread21(u) << (2 - k);
+    }
+    return code;
+}
+
+__global__ void k_morton(const Box* box, const uint32_t* ids, uint32_t m, const unsigned long long* b,
+                         unsigned long long* code, uint32_t* vals) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
         uint32_t id = ids[i];
         const Box& q = box[id];
-        unsigned long long c = 0;
-        for (int k = 0; k < 3; ++k) {
-            double t = ext[k] > 0.0 ? (0.5 * (q.lo[k] + q.hi[k]) - lo[k]) / ext[k] : 0.0;
-            double s = t * 2097152.0;
-            unsigned long long u = s <= 0.0 ? 0ull : (s >= 2097151.0 ? 2097151ull : (unsigned long long)s);
-            c |= spread21(u) << (2 - k);
-        }
-        code[i] = c;
+        double c[3] = {0.5 * (q.lo[0] + q.hi[0]), 0.5 * (q.lo[1] + q.hi[1]), 0.5 * (q.lo[2] + q.hi[2])};
+        code[i] = morton63(c, b);
         vals[i] = id;
+    }
+}
+
+// Bounds and Morton codes of points (the VF query order).
+__global__ void k_point_bounds(const double4* x, uint32_t n, unsigned long long* b) {
+    unsigned long long lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0, 0, 0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double4 p = x[i];
+        double c[3] = {p.x, p.y, p.z};
+        for (int k = 0; k < 3; ++k) {
+            unsigned long long key = order_key(c[k]);
+            lo[k] = min(lo[k], key);
+            hi[k] = max(hi[k], key);
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&b[k], lo[k]);
+            atomicMax(&b[3 + k], hi[k]);
+        }
+    }
+}
+
+__global__ void k_point_morton(const double4* x, uint32_t n, const unsigned long long* b, unsigned long long* code,
+                               uint32_t* vals) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double4 p = x[i];
+        double c[3] = {p.x, p.y, p.z};
+        code[i] = morton63(c, b);
+        vals[i] = i;
     }
 }
 
@@ -148,8 +181,10 @@ __device__ __forceinline__ int lbvh_delta(const unsigned long long* code, int m,
     return __clzll(a ^ b);
 }
 
-// Karras 2012, "Maximizing parallelism in the construction of BVHs".
-__global__ void k_karras(const unsigned long long* code, int m, int2* child, int* parent) {
+// Karras 2012, "Maximizing parallelism in the construction of BVHs". The
+// children go into the node records (d.x, d.y); the boxes follow in
+// k_lbvh_refit.
+__global__ void k_karras(const unsigned long long* code, int m, LNode* node, int* parent) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m - 1; i += gridDim.x * blockDim.x) {
         int d = (lbvh_delta(code, m, i, i + 1) - lbvh_delta(code, m, i, i - 1)) >= 0 ? 1 : -1;
         int dmin = lbvh_delta(code, m, i, i - d);
@@ -182,118 +217,184 @@ __global__ void k_karras(const unsigned long long* code, int m, int2* child, int
             right = gamma + 1;
             parent[gamma + 1] = i;
         }
-        child[i] = make_int2(left, right);
+        *reinterpret_cast<int2*>(&node[i].d) = make_int2(left, right);
         if (i == 0) parent[0] = -1;
     }
 }
 
-__global__ void k_lbvh_boxes(const Box* prim_box, const uint32_t* leaf_prim, int m, const int2* child,
-                             const int* parent, unsigned* visits, Box* node_box, uint32_t* node_max) {
+__global__ void k_leaf_boxes(const Box* prim_box, const uint32_t* leaf_prim, int m, Box* leaf_box) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+        leaf_box[i] = prim_box[leaf_prim[i]];
+}
+
+// Writes one child's box and largest id into its parent's record (slot 0 =
+// left: floats 0..5 and d.z; slot 1 = right: floats 6..11 and d.w).
+__device__ __forceinline__ void put_slot(LNode* node, int p, int slot, const float* lo, const float* hi, uint32_t mx) {
+    float* f = reinterpret_cast<float*>(node + p) + 6 * slot;
+    f[0] = lo[0];
+    f[1] = lo[1];
+    f[2] = lo[2];
+    f[3] = hi[0];
+    f[4] = hi[1];
+    f[5] = hi[2];
+    reinterpret_cast<int*>(&node[p].d)[2 + slot] = (int)mx;
+}
+
+// Bottom-up boxes: each leaf writes its outward-rounded box into its parent's
+// slot; the second of a node's two children to arrive (atomic counter) forms
+// the node's box from both slots and carries it one level up. FP32 min/max of
+// outward-rounded boxes is exact, so every node box contains the exact boxes
+// below it.
+__global__ void k_lbvh_refit(const Box* leaf_box, const uint32_t* leaf_prim, int m, LNode* node, const int* parent,
+                             unsigned* visits) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x) {
-        int node = parent[m - 1 + i];
-        while (node >= 0) {
+        const Box& b = leaf_box[i];
+        float lo[3], hi[3];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = __double2float_rd(b.lo[k]);
+            hi[k] = __double2float_ru(b.hi[k]);
+        }
+        uint32_t mx = leaf_prim[i];
+        int code = i | 0x80000000;
+        int p = parent[m - 1 + i];
+        while (p >= 0) {
+            int2 ch = *reinterpret_cast<const int2*>(&node[p].d);
+            put_slot(node, p, ch.x == code ? 0 : 1, lo, hi, mx);
             __threadfence();
-            if (atomicAdd(&visits[node], 1u) == 0u) break;
-            int2 c = child[node];
-            Box a = (c.x & 0x80000000) ? prim_box[leaf_prim[c.x & 0x7fffffff]] : ldcg_box(&node_box[c.x]);
-            Box b = (c.y & 0x80000000) ? prim_box[leaf_prim[c.y & 0x7fffffff]] : ldcg_box(&node_box[c.y]);
-            uint32_t ma = (c.x & 0x80000000) ? leaf_prim[c.x & 0x7fffffff] : __ldcg(&node_max[c.x]);
-            uint32_t mb = (c.y & 0x80000000) ? leaf_prim[c.y & 0x7fffffff] : __ldcg(&node_max[c.y]);
-            node_box[node] = box_union(a, b);
-            node_max[node] = max(ma, mb);
-            node = parent[node];
+            if (atomicAdd(&visits[p], 1u) == 0u) break;
+            __threadfence();
+            const float* f = reinterpret_cast<const float*>(node + p);
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = fminf(__ldcg(f + k), __ldcg(f + 6 + k));
+                hi[k] = fmaxf(__ldcg(f + 3 + k), __ldcg(f + 9 + k));
+            }
+            const int* d = reinterpret_cast<const int*>(&node[p].d);
+            mx = max((uint32_t)__ldcg(d + 2), (uint32_t)__ldcg(d + 3));
+            code = p;
+            p = parent[p];
         }
     }
 }
 
 int Lbvh::build(const Box* prim_box, const uint32_t* ids, uint32_t count, cudaStream_t s, unsigned int* err) {
     m = count;
+    built = true;
     if (m == 0) return 0;
     leaf_prim.reserve(m);
     ids_tmp.reserve(m);
     morton.reserve(m);
     morton_tmp.reserve(m);
     bounds.reserve(6);
-    node_box.reserve(m > 1 ? m - 1 : 1);
-    node_max.reserve(m > 1 ? m - 1 : 1);
-    child.reserve(m > 1 ? m - 1 : 1);
+    node.reserve(m > 1 ? m - 1 : 1);
     parent.reserve(2 * m);
     visits.reserve(m);
+    leaf_box.reserve(m);
     k_bounds_init<<<1, 32, 0, s>>>(bounds.ptr);
     k_centroid_bounds<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr);
     k_morton<<<grid_for(m, 256), 256, 0, s>>>(prim_box, ids, m, bounds.ptr, morton_tmp.ptr, ids_tmp.ptr);
     int sorts = sorter.sort_pairs(morton_tmp.ptr, morton.ptr, ids_tmp.ptr, leaf_prim.ptr, m, 63, s, err, DERR_SORT_WAIT);
+    int n = 3 + sorts;
     if (m > 1) {
-        k_karras<<<grid_for(m - 1, 256), 256, 0, s>>>(morton.ptr, (int)m, child.ptr, parent.ptr);
-        CC_CUDA(cudaMemsetAsync(visits.ptr, 0, (m - 1) * sizeof(unsigned), s));
-        k_lbvh_boxes<<<grid_for(m, 256), 256, 0, s>>>(prim_box, leaf_prim.ptr, (int)m, child.ptr, parent.ptr,
-                                                      visits.ptr, node_box.ptr, node_max.ptr);
+        k_karras<<<grid_for(m - 1, 256), 256, 0, s>>>(morton.ptr, (int)m, node.ptr, parent.ptr);
+        ++n;
     }
     CC_CUDA(cudaGetLastError());
-    return (m > 1 ? 5 : 3) + sorts;
+    return n + refit(prim_box, s);
 }
 
-// Stack traversal over the primitives with id > `above` only: subtrees whose
-// largest primitive id is <= above are skipped unvisited (self-pair queries
-// that keep the canonical order e < f). Otherwise as lbvh_traverse.
-template <class NodeOk, class LeafOk, class Visit>
-__device__ __forceinline__ bool lbvh_traverse_above(const LbvhView& t, uint32_t above, NodeOk node_ok, LeafOk leaf_ok,
-                                                    Visit visit) {
+int Lbvh::refit(const Box* prim_box, cudaStream_t s) {
+    if (m == 0) return 0;
+    k_leaf_boxes<<<grid_for(m, 256), 256, 0, s>>>(prim_box, leaf_prim.ptr, (int)m, leaf_box.ptr);
+    if (m > 1) {
+        CC_CUDA(cudaMemsetAsync(visits.ptr, 0, (m - 1) * sizeof(unsigned), s));
+        k_lbvh_refit<<<grid_for(m, 256), 256, 0, s>>>(leaf_box.ptr, leaf_prim.ptr, (int)m, node.ptr, parent.ptr,
+                                                      visits.ptr);
+    }
+    CC_CUDA(cudaGetLastError());
+    return m > 1 ? 2 : 1;
+}
+
+// A query box rounded outward to FP32 for the node tests.
+struct QBox {
+    float lo[3], hi[3];
+};
+__device__ __forceinline__ QBox qbox(const Box& b) {
+    QBox q;
+    for (int k = 0; k < 3; ++k) {
+        q.lo[k] = __double2float_rd(b.lo[k]);
+        q.hi[k] = __double2float_ru(b.hi[k]);
+    }
+    return q;
+}
+
+// Node test for a distance query: false only if the exact distance between
+// the query's and the child's FP64 boxes exceeds the search radius. The gaps
+// and their squares are rounded down and the bound (r2_up) up, so the test
+// never drops a child whose leaves pass the exact FP64 leaf test.
+__device__ __forceinline__ bool near32(const QBox& q, float lx, float ly, float lz, float hx, float hy, float hz,
+                                       float r2_up) {
+    float gx = fmaxf(0.f, fmaxf(__fsub_rd(lx, q.hi[0]), __fsub_rd(q.lo[0], hx)));
+    float gy = fmaxf(0.f, fmaxf(__fsub_rd(ly, q.hi[1]), __fsub_rd(q.lo[1], hy)));
+    float gz = fmaxf(0.f, fmaxf(__fsub_rd(lz, q.hi[2]), __fsub_rd(q.lo[2], hz)));
+    float d2 = __fadd_rd(__fadd_rd(__fmul_rd(gx, gx), __fmul_rd(gy, gy)), __fmul_rd(gz, gz));
+    return d2 <= r2_up;
+}
+// the bound for near32: search^2 with a 1e-6 relative margin for the FP64
+// rounding of the exact leaf test, rounded up to FP32
+__device__ __forceinline__ float r2_bound(double search2) { return __double2float_ru(search2 * (1.0 + 1e-6)); }
+
+// Node test for an overlap query (outward-rounded boxes overlap whenever the
+// exact ones do).
+__device__ __forceinline__ bool overlap32(const QBox& q, float lx, float ly, float lz, float hx, float hy, float hz) {
+    return !(lx > q.hi[0] || ly > q.hi[1] || lz > q.hi[2] || hx < q.lo[0] || hy < q.lo[1] || hz < q.lo[2]);
+}
+
+// Depth-first traversal that goes down one passing child and stacks the
+// other. near(lx, ly, lz, hx, hy, hz) tests a child's FP32 box; leaf_ok(box)
+// is the exact FP64 primitive predicate; visit(prim) receives the accepted
+// primitive id. With ABOVE, only primitives with id > above are visited and
+// subtrees whose largest id is <= above are skipped unvisited (self-pair
+// queries that keep the canonical order e < f). Returns false if the stack
+// overflowed.
+constexpr int kTraversalStack = 96;
+template <bool ABOVE, class Near, class LeafOk, class Visit>
+__device__ __forceinline__ bool lbvh_walk(const LbvhView& t, uint32_t above, Near near, LeafOk leaf_ok, Visit visit) {
     if (t.m == 0) return true;
     if (t.m == 1) {
         uint32_t p = t.leaf_prim[0];
-        if (p > above && leaf_ok(t.prim_box[p])) visit(p);
+        if ((!ABOVE || p > above) && leaf_ok(t.leaf_box[0])) visit(p);
         return true;
     }
-    int stack[96];
+    int stack[kTraversalStack];
     int sp = 0;
-    if (t.node_max[0] <= above || !node_ok(t.node_box[0])) return true;
-    stack[sp++] = 0;
-    while (sp > 0) {
-        int node = stack[--sp];
-        int2 c = t.child[node];
-        int cs[2] = {c.x, c.y};
-        for (int k = 0; k < 2; ++k) {
-            int ch = cs[k];
-            if (ch & 0x80000000) {
-                uint32_t p = t.leaf_prim[ch & 0x7fffffff];
-                if (p > above && leaf_ok(t.prim_box[p])) visit(p);
-            } else if (t.node_max[ch] > above && node_ok(t.node_box[ch])) {
-                if (sp >= 96) return false;
-                stack[sp++] = ch;
-            }
+    int node = 0;
+    while (true) {
+        const float4* r = reinterpret_cast<const float4*>(t.node + node);
+        const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
+        const int4 d = __ldg(reinterpret_cast<const int4*>(r + 3));
+        bool go_l = (!ABOVE || (uint32_t)d.z > above) && near(a.x, a.y, a.z, a.w, b.x, b.y);
+        bool go_r = (!ABOVE || (uint32_t)d.w > above) && near(b.z, b.w, c.x, c.y, c.z, c.w);
+        if (go_l && d.x < 0) {
+            uint32_t i = (uint32_t)d.x & 0x7fffffffu;
+            if (leaf_ok(t.leaf_box[i])) visit(t.leaf_prim[i]);
+            go_l = false;
         }
-    }
-    return true;
-}
-
-// Stack traversal. node_ok(box) prunes internal nodes; leaf_ok(box) is the
-// exact primitive predicate; visit(prim) receives the accepted primitive id.
-template <class NodeOk, class LeafOk, class Visit>
-__device__ __forceinline__ bool lbvh_traverse(const LbvhView& t, NodeOk node_ok, LeafOk leaf_ok, Visit visit) {
-    if (t.m == 0) return true;
-    if (t.m == 1) {
-        uint32_t p = t.leaf_prim[0];
-        if (leaf_ok(t.prim_box[p])) visit(p);
-        return true;
-    }
-    int stack[96];
-    int sp = 0;
-    if (!node_ok(t.node_box[0])) return true;
-    stack[sp++] = 0;
-    while (sp > 0) {
-        int node = stack[--sp];
-        int2 c = t.child[node];
-        int cs[2] = {c.x, c.y};
-        for (int k = 0; k < 2; ++k) {
-            int ch = cs[k];
-            if (ch & 0x80000000) {
-                uint32_t p = t.leaf_prim[ch & 0x7fffffff];
-                if (leaf_ok(t.prim_box[p])) visit(p);
-            } else if (node_ok(t.node_box[ch])) {
-                if (sp >= 96) return false;
-                stack[sp++] = ch;
-            }
+        if (go_r && d.y < 0) {
+            uint32_t i = (uint32_t)d.y & 0x7fffffffu;
+            if (leaf_ok(t.leaf_box[i])) visit(t.leaf_prim[i]);
+            go_r = false;
+        }
+        if (go_l && go_r) {
+            if (sp >= kTraversalStack) return false;
+            stack[sp++] = d.y;
+            node = d.x;
+        } else if (go_l) {
+            node = d.x;
+        } else if (go_r) {
+            node = d.y;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
         }
     }
     return true;
@@ -514,12 +615,21 @@ __device__ __forceinline__ unsigned long long append_slot(unsigned long long* co
 
 // VF candidates (candidates.rs:29-37): every point against triangles, pairs
 // with box distance <= search, not both fixed, triangle not adjacent.
-__global__ void k_vf_query(WorldView w, LbvhView tri_moving, LbvhView tri_fixed, double search2, uint2* out,
-                           unsigned long long cap, unsigned long long* count, unsigned int* err) {
-    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < w.n_all; v += gridDim.x * blockDim.x) {
+// Points are taken in `order` (a Morton order of the points), so that the
+// lanes of a warp walk nearby points. (Walking a warp's 32 queries as one
+// node sequence, the union of their walks, measured 4x slower for VF and
+// 1.2x for EE on the fold: the union is several times the longest walk.)
+__global__ void k_vf_query(WorldView w, const uint32_t* order, LbvhView tri_moving, LbvhView tri_fixed, double search2,
+                           uint2* out, unsigned long long cap, unsigned long long* count, unsigned int* err) {
+    const float r2 = r2_bound(search2);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < w.n_all; j += gridDim.x * blockDim.x) {
+        const uint32_t v = order[j];
         Box q;
         box_of1(ld3(w.x, v), q);
-        auto node_ok = [&](const Box& b) { return !(box_dist2(q, b) > search2); };
+        const QBox q32 = qbox(q);
+        auto near = [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+            return near32(q32, lx, ly, lz, hx, hy, hz, r2);
+        };
         auto leaf_ok = [&](const Box& b) { return box_dist2(q, b) <= search2; };
         auto visit = [&](uint32_t t) {
             uint3 ids = w.tri[t];
@@ -527,23 +637,29 @@ __global__ void k_vf_query(WorldView w, LbvhView tri_moving, LbvhView tri_fixed,
             unsigned long long k = append_slot(count);
             if (k < cap) out[k] = make_uint2(v, t);
         };
-        bool ok = lbvh_traverse(tri_moving, node_ok, leaf_ok, visit);
-        if (v < w.moving) ok = lbvh_traverse(tri_fixed, node_ok, leaf_ok, visit) && ok;
+        bool ok = lbvh_walk<false>(tri_moving, 0u, near, leaf_ok, visit);
+        if (v < w.moving) ok = lbvh_walk<false>(tri_fixed, 0u, near, leaf_ok, visit) && ok;
         if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
     }
 }
 
 // EE candidates (candidates.rs:38-55): moving edges against moving edges
 // (each unordered pair once, canonical e < f) and against fixed edges
-// (moving edge first).
+// (moving edge first). `edge_moving` lists the moving edges in the moving
+// edge tree's leaf order (a Morton order), so neighbouring lanes query
+// neighbouring edges.
 __global__ void k_ee_query(WorldView w, const uint32_t* edge_moving, uint32_t n_moving_edges, LbvhView edge_moving_t,
                            LbvhView edge_fixed_t, double search2, uint2* out, unsigned long long cap,
                            unsigned long long* count, unsigned int* err) {
+    const float r2 = r2_bound(search2);
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_moving_edges; k += gridDim.x * blockDim.x) {
         uint32_t e = edge_moving[k];
         Box q = w.edge_box[e];
+        const QBox q32 = qbox(q);
         uint2 ids = w.edges[e];
-        auto node_ok = [&](const Box& b) { return !(box_dist2(q, b) > search2); };
+        auto near = [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+            return near32(q32, lx, ly, lz, hx, hy, hz, r2);
+        };
         auto leaf_ok = [&](const Box& b) { return box_dist2(q, b) <= search2; };
         auto filtered = [&](uint32_t f) {
             uint2 js = w.edges[f];
@@ -560,64 +676,57 @@ __global__ void k_ee_query(WorldView w, const uint32_t* edge_moving, uint32_t n_
             unsigned long long i = append_slot(count);
             if (i < cap) out[i] = make_uint2(e, f);
         };
-        bool ok = lbvh_traverse_above(edge_moving_t, e, node_ok, leaf_ok, visit_moving);
-        ok = lbvh_traverse(edge_fixed_t, node_ok, leaf_ok, visit_fixed) && ok;
+        bool ok = lbvh_walk<true>(edge_moving_t, e, near, leaf_ok, visit_moving);
+        ok = lbvh_walk<false>(edge_fixed_t, 0u, near, leaf_ok, visit_fixed) && ok;
         if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
     }
 }
 
 // ------------------------------------------------------------ narrow phase
-// Contact keys: hi = kind << 2nb | v0 << nb | v1, lo = v2 << nb | v3, with nb
-// bits per vertex id (2^nb >= vertex count): lexicographic (kind, v0..v3)
-// order in as few radix digits as the ids need.
-__device__ __forceinline__ void push_contact(unsigned kind, uint32_t i0, uint32_t i1, uint32_t i2, uint32_t i3,
-                                             double eps, unsigned long long* hi, unsigned long long* lo,
-                                             double* epsv, uint32_t* idx, unsigned long long cap,
-                                             unsigned long long* count, uint32_t nb) {
-    // canonical vertex order (world.rs:435-452)
-    uint32_t v[4] = {i0, i1, i2, i3};
-    auto sw = [&](int a, int b) {
-        uint32_t t = v[a];
-        v[a] = v[b];
-        v[b] = t;
-    };
-    if (kind == 0 && v[0] > v[1]) sw(0, 1);
-    if (kind == 1 && v[1] > v[2]) sw(1, 2);
-    if (kind == 2) {
-        if (v[1] > v[2]) sw(1, 2);
-        if (v[2] > v[3]) sw(2, 3);
-        if (v[1] > v[2]) sw(1, 2);
-    }
-    if (kind == 3) {
-        if (v[0] > v[1]) sw(0, 1);
-        if (v[2] > v[3]) sw(2, 3);
-        if (v[0] > v[2]) {
-            sw(0, 2);
-            sw(1, 3);
-        }
-    }
-    unsigned long long k = append_slot(count);
-    if (k < cap) {
-        hi[k] = ((unsigned long long)kind << (2 * nb)) | ((unsigned long long)v[0] << nb) | (unsigned long long)v[1];
-        lo[k] = ((unsigned long long)v[2] << nb) | (unsigned long long)v[3];
-        epsv[k] = eps;
-        idx[k] = (uint32_t)k;
-    }
-}
-
+// Contact keys. The reference orders contacts by (kind, v0, v1, v2, v3) with
+// the vertices in canonical order (world.rs:435-452). Within a kind the
+// trailing vertices always form a mesh edge (PE: v1 v2; EE: v0 v1 and v2 v3)
+// or a triangle (PF: v1 v2 v3), so each such group is replaced by its rank
+// among the mesh's distinct edges (or triangles) in lexicographic vertex
+// order, which keeps the order:
+//   PP (v0, v1)          -> (v0, v1)
+//   PE (v0, v1, v2)      -> (v0, rank(v1 v2))
+//   PF (v0, v1, v2, v3)  -> (v0, rank(v1 v2 v3))
+//   EE (v0, v1, v2, v3)  -> (rank(v0 v1), rank(v2 v3))
+// key = kind << 2W | A << W | B with 2^W above every vertex id and rank: one
+// key of 2W + 2 bits, sorted in one keys-only radix sort.
 struct NarrowOut {
-    unsigned long long* hi;
-    unsigned long long* lo;
-    double* eps;
-    uint32_t* idx;
+    unsigned long long* key;
     unsigned long long cap;
     unsigned long long* count;
     unsigned long long* dist;  // [n_all] double bits
     unsigned long long* vf_count;
     unsigned long long* ee_count;
     unsigned long long* rejections;
-    uint32_t nb;  // bits per vertex id in the contact keys
+    const uint32_t* edge_rank;  // [n_edge]
+    const uint32_t* tri_rank;   // [n_tri]
+    uint32_t w;                 // bits per key field
 };
+
+__device__ __forceinline__ void push_key(const NarrowOut& o, unsigned kind, uint32_t a, uint32_t b) {
+    unsigned long long k = append_slot(o.count);
+    if (k < o.cap)
+        o.key[k] = ((unsigned long long)kind << (2 * o.w)) | ((unsigned long long)a << o.w) | (unsigned long long)b;
+}
+__device__ __forceinline__ void push_pp(const NarrowOut& o, uint32_t i, uint32_t j) {
+    push_key(o, 0, min(i, j), max(i, j));
+}
+// point v against mesh edge e
+__device__ __forceinline__ void push_pe(const NarrowOut& o, uint32_t v, uint32_t e) { push_key(o, 1, v, o.edge_rank[e]); }
+// point v against triangle t
+__device__ __forceinline__ void push_pf(const NarrowOut& o, uint32_t v, uint32_t t) { push_key(o, 2, v, o.tri_rank[t]); }
+// edges e (vertices ids) and f (js), the canonical order putting first the
+// edge with the smaller first vertex (world.rs:446-451)
+__device__ __forceinline__ void push_ee(const NarrowOut& o, uint32_t e, uint2 ids, uint32_t f, uint2 js) {
+    uint32_t re = o.edge_rank[e], rf = o.edge_rank[f];
+    if (ids.x > js.x) push_key(o, 3, rf, re);
+    else push_key(o, 3, re, rf);
+}
 
 __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, const uint2* ee,
                          unsigned long long n_ee, double query_radius, const unsigned long long* max_abs_bits,
@@ -653,15 +762,11 @@ __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, 
             atomicMin(&o.dist[ids.y], db);
             atomicMin(&o.dist[ids.z], db);
             if (kind == 0) {
-                if (vertex_feasible(w, xv, fid))
-                    push_contact(0, v, fid, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
+                if (vertex_feasible(w, xv, fid)) push_pp(o, v, fid);
             } else if (kind == 1) {
-                if (edge_feasible(w, xv, fid)) {
-                    uint2 ev = w.edges[fid];
-                    push_contact(1, v, ev.x, ev.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
-                }
+                if (edge_feasible(w, xv, fid)) push_pe(o, v, fid);
             } else {
-                push_contact(2, v, ids.x, ids.y, ids.z, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
+                push_pf(o, v, t);
             }
         } else {
             unsigned long long kk = k - n_vf;
@@ -689,16 +794,10 @@ __global__ void k_narrow(WorldView w, const uint2* vf, unsigned long long n_vf, 
             if ((end_a >= 0 && !vertex_feasible(w, q, (uint32_t)end_a)) ||
                 (end_b >= 0 && !vertex_feasible(w, p, (uint32_t)end_b)))
                 continue;
-            if (end_a >= 0 && end_b >= 0)
-                push_contact(0, (uint32_t)end_a, (uint32_t)end_b, 0, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap,
-                             o.count, o.nb);
-            else if (end_a >= 0)
-                push_contact(1, (uint32_t)end_a, js.x, js.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
-            else if (end_b >= 0)
-                push_contact(1, (uint32_t)end_b, ids.x, ids.y, 0, 0.0, o.hi, o.lo, o.eps, o.idx, o.cap, o.count, o.nb);
-            else
-                push_contact(3, ids.x, ids.y, js.x, js.y, 1e-3 * w.rest_len2[e] * w.rest_len2[f], o.hi, o.lo, o.eps,
-                             o.idx, o.cap, o.count, o.nb);
+            if (end_a >= 0 && end_b >= 0) push_pp(o, (uint32_t)end_a, (uint32_t)end_b);
+            else if (end_a >= 0) push_pe(o, (uint32_t)end_a, f);
+            else if (end_b >= 0) push_pe(o, (uint32_t)end_b, e);
+            else push_ee(o, e, ids, f, js);
         }
     }
     for (int s = 16; s > 0; s >>= 1) {
@@ -717,14 +816,9 @@ __global__ void k_fill_u64(unsigned long long* p, size_t n, unsigned long long v
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
 
-__global__ void k_gather_u64(const unsigned long long* src, const uint32_t* idx, unsigned long long* dst, size_t n) {
+__global__ void k_unique_flags(const unsigned long long* key, size_t n, uint32_t* flag) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        dst[i] = src[idx[i]];
-}
-
-__global__ void k_unique_flags(const unsigned long long* hi, const unsigned long long* lo, size_t n, uint32_t* flag) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        flag[i] = (i == 0 || hi[i] != hi[i - 1] || lo[i] != lo[i - 1]) ? 1u : 0u;
+        flag[i] = (i == 0 || key[i] != key[i - 1]) ? 1u : 0u;
 }
 
 __device__ __forceinline__ uint32_t kind_count(uint32_t kind) { return kind == 0 ? 2u : (kind == 1 ? 3u : 4u); }
@@ -757,17 +851,50 @@ __device__ bool contact_active(const WorldView& w, uint32_t kind, uint4 v, doubl
     return true;
 }
 
-__global__ void k_compact(const unsigned long long* hi, const unsigned long long* lo, const uint32_t* idx_sorted,
-                          const double* raw_eps, const uint32_t* flag, const uint32_t* pos, size_t n,
-                          uint32_t* c_kind, uint4* c_verts, double* c_eps, uint32_t nb) {
-    const unsigned long long m = (1ull << nb) - 1ull;
+// Rank tables for decoding contact keys: the distinct edges and triangles in
+// lexicographic vertex order.
+struct RankTables {
+    const uint2* edge_verts;    // [edge ranks] (v0 < v1)
+    const uint32_t* edge_id;    // [edge ranks] the world edge of each rank
+    const uint3* tri_verts;     // [triangle ranks] (v1 < v2 < v3)
+};
+
+// Unique keys back to (kind, vertices, epsilon). The EE mollifier epsilon is
+// 1e-3 |e0|^2 |f0|^2 (world.rs:174-178) in the operand order of the candidate
+// pair that found the contact: moving-moving pairs have e < f by edge id,
+// moving-fixed pairs the moving edge first (k_ee_query); each unordered edge
+// pair is a candidate once, so that order is a function of the two edges.
+__global__ void k_compact(WorldView w, const unsigned long long* key, const uint32_t* flag, const uint32_t* pos,
+                          size_t n, RankTables r, uint32_t bits, uint32_t* c_kind, uint4* c_verts, double* c_eps) {
+    const unsigned long long m = (1ull << bits) - 1ull;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!flag[i]) continue;
-        uint32_t j = pos[i];
-        unsigned long long h = hi[i], l = lo[i];
-        c_kind[j] = (uint32_t)(h >> (2 * nb));
-        c_verts[j] = make_uint4((uint32_t)((h >> nb) & m), (uint32_t)(h & m), (uint32_t)(l >> nb), (uint32_t)(l & m));
-        c_eps[j] = raw_eps[idx_sorted[i]];
+        const uint32_t j = pos[i];
+        const unsigned long long k = key[i];
+        const uint32_t kind = (uint32_t)(k >> (2 * bits));
+        const uint32_t a = (uint32_t)((k >> bits) & m), b = (uint32_t)(k & m);
+        uint4 v = make_uint4(0, 0, 0, 0);
+        double eps = 0.0;
+        if (kind == 0) {
+            v = make_uint4(a, b, 0, 0);
+        } else if (kind == 1) {
+            uint2 e = r.edge_verts[b];
+            v = make_uint4(a, e.x, e.y, 0);
+        } else if (kind == 2) {
+            uint3 t = r.tri_verts[b];
+            v = make_uint4(a, t.x, t.y, t.z);
+        } else {
+            uint2 e = r.edge_verts[a], f = r.edge_verts[b];
+            v = make_uint4(e.x, e.y, f.x, f.y);
+            uint32_t ea = r.edge_id[a], eb = r.edge_id[b];
+            bool ma = e.x < w.moving, mb = f.x < w.moving;  // an edge moves if its smaller vertex does
+            uint32_t first = (ma && mb) ? min(ea, eb) : (ma ? ea : eb);
+            uint32_t second = first == ea ? eb : ea;
+            eps = 1e-3 * w.rest_len2[first] * w.rest_len2[second];
+        }
+        c_kind[j] = kind;
+        c_verts[j] = v;
+        c_eps[j] = eps;
     }
 }
 
@@ -874,10 +1001,13 @@ __global__ void k_intersections(WorldView w, LbvhView tri_moving, LbvhView tri_f
             }
             if (hit) atomicMin(first_hit, ((unsigned long long)i << 32) | j);
         };
-        auto node_ok = [&](const Box& b) { return box_overlap(b, q); };
+        const QBox q32 = qbox(q);
+        auto near = [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+            return overlap32(q32, lx, ly, lz, hx, hy, hz);
+        };
         auto leaf_ok = [&](const Box& b) { return box_overlap(b, q); };
-        bool ok = lbvh_traverse(tri_moving, node_ok, leaf_ok, visit);
-        if (!t_fixed) ok = lbvh_traverse(tri_fixed, node_ok, leaf_ok, visit) && ok;
+        bool ok = lbvh_walk<false>(tri_moving, 0u, near, leaf_ok, visit);
+        if (!t_fixed) ok = lbvh_walk<false>(tri_fixed, 0u, near, leaf_ok, visit) && ok;
         if (!ok) atomicOr(err, DERR_STACK_OVERFLOW);
     }
 }
@@ -957,6 +1087,45 @@ World::World(const double* x_all, size_t n_all, const std::vector<std::array<uin
     }
     std::vector<double> rl2(n_edge_);
     for (size_t e = 0; e < n_edge_; ++e) rl2[e] = len2(X(top_.edges[e][0]) - X(top_.edges[e][1]));
+    // contact-key ranks: distinct edges and triangles (vertex sets) in
+    // lexicographic order; equal sets share a rank
+    std::vector<uint32_t> edge_rank(n_edge_), tri_rank(n_tri_), rank_edge_id;
+    std::vector<uint2> rank_edge_verts;
+    std::vector<uint3> rank_tri_verts;
+    {
+        std::vector<uint32_t> ord(n_edge_);
+        for (size_t e = 0; e < n_edge_; ++e) ord[e] = (uint32_t)e;
+        std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+            return top_.edges[a] < top_.edges[b] || (top_.edges[a] == top_.edges[b] && a < b);
+        });
+        for (size_t k = 0; k < n_edge_; ++k) {
+            const auto& ev = top_.edges[ord[k]];
+            if (k == 0 || ev != top_.edges[ord[k - 1]]) {
+                rank_edge_verts.push_back(make_uint2(ev[0], ev[1]));
+                rank_edge_id.push_back(ord[k]);
+            }
+            edge_rank[ord[k]] = (uint32_t)rank_edge_verts.size() - 1;
+        }
+        std::vector<std::array<uint32_t, 3>> sorted(n_tri_);
+        for (size_t t = 0; t < n_tri_; ++t) {
+            sorted[t] = top_.tri[t];
+            std::sort(sorted[t].begin(), sorted[t].end());
+        }
+        std::vector<uint32_t> tord(n_tri_);
+        for (size_t t = 0; t < n_tri_; ++t) tord[t] = (uint32_t)t;
+        std::sort(tord.begin(), tord.end(), [&](uint32_t a, uint32_t b) {
+            return sorted[a] < sorted[b] || (sorted[a] == sorted[b] && a < b);
+        });
+        for (size_t k = 0; k < n_tri_; ++k) {
+            const auto& tv = sorted[tord[k]];
+            if (k == 0 || tv != sorted[tord[k - 1]]) rank_tri_verts.push_back(make_uint3(tv[0], tv[1], tv[2]));
+            tri_rank[tord[k]] = (uint32_t)rank_tri_verts.size() - 1;
+        }
+    }
+    key_bits_ = 1;
+    while ((1ull << key_bits_) < std::max<uint64_t>({(uint64_t)n_all_, rank_edge_verts.size(), rank_tri_verts.size()}))
+        ++key_bits_;
+    if (key_bits_ > 31) throw Failure{CC_ERR_INVALID_ARGUMENT, "OGC: more than 2^31 vertices, edges or triangles"};
     for (size_t t = 0; t < n_tri_; ++t) {
         const auto& v = top_.tri[t];
         (v[0] < moving || v[1] < moving || v[2] < moving ? tri_moving_h_ : tri_fixed_h_).push_back((uint32_t)t);
@@ -987,6 +1156,11 @@ World::World(const double* x_all, size_t n_all, const std::vector<std::array<uin
     ex_off_.upload(ex_off, stream_);
     ex_.upload(exv, stream_);
     rest_len2_.upload(rl2, stream_);
+    edge_rank_.upload(edge_rank, stream_);
+    tri_rank_.upload(tri_rank, stream_);
+    rank_edge_verts_.upload(rank_edge_verts, stream_);
+    rank_edge_id_.upload(rank_edge_id, stream_);
+    rank_tri_verts_.upload(rank_tri_verts, stream_);
     x_.upload(xh, stream_);
     fixed_x_.upload(xh.data() + moving, n_all - moving, stream_);
     tri_box_.reserve(n_tri_);
@@ -1005,6 +1179,9 @@ World::World(const double* x_all, size_t n_all, const std::vector<std::array<uin
     stats_d_.reserve(1);
     stats_h_.reserve(1);
     std::memset(stats_h_.ptr, 0, sizeof(DetectStats));
+    CC_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+    CC_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+    CC_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
     // fixed trees are built once: fixed geometry never moves
     stats_d_.zero(1, stream_);
     refit(false);
@@ -1016,6 +1193,9 @@ World::World(const double* x_all, size_t n_all, const std::vector<std::array<uin
 World::~World() {
     for (cudaEvent_t e : phase_ev_)
         if (e) cudaEventDestroy(e);
+    if (fork_) cudaEventDestroy(fork_);
+    if (join_) cudaEventDestroy(join_);
+    if (side_) cudaStreamDestroy(side_);
 }
 
 WorldView World::view() const {
@@ -1062,13 +1242,54 @@ static void raise_device_error(unsigned int e) {
     if (e & DERR_SORT_WAIT) throw Failure{CC_ERR_DEVICE_TIMEOUT, "OGC radix sort look-back wait gave up"};
 }
 
+// The moving trees for the current primitive boxes: the triangle tree on the
+// side stream, the edge tree on the main one (after fork_, recorded here, the
+// side stream waits for the boxes). The caller joins the streams.
+int World::update_trees() {
+    bool build = !tree_tri_moving_.built || !tree_edge_moving_.built;
+    if (!build && tree_period_ > 0 && rebuilds_since_build_ + 1 >= tree_period_) build = true;
+    if (build) {
+        rebuilds_since_build_ = 0;
+        ++tree_builds_;
+    } else {
+        ++rebuilds_since_build_;
+    }
+    CC_CUDA(cudaEventRecord(fork_, stream_));
+    CC_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
+    unsigned int* err = &stats_d_.ptr->error;
+    int n = build ? tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), side_, err)
+                  : tree_tri_moving_.refit(tri_box_.ptr, side_);
+    n += build ? tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_, err)
+               : tree_edge_moving_.refit(edge_box_.ptr, stream_);
+    if (build) n += order_points();
+    return n;
+}
+
+// A Morton order of all points (the VF queries' order), from the current
+// positions; refreshed with the trees' topology.
+int World::order_points() {
+    const uint32_t n = (uint32_t)n_all_;
+    if (n == 0) return 0;
+    pt_bounds_.reserve(6);
+    pt_code_.reserve(n);
+    pt_code_s_.reserve(n);
+    pt_ids_.reserve(n);
+    point_order_.reserve(n);
+    k_bounds_init<<<1, 32, 0, stream_>>>(pt_bounds_.ptr);
+    k_point_bounds<<<grid_for(n, 256), 256, 0, stream_>>>(x_.ptr, n, pt_bounds_.ptr);
+    k_point_morton<<<grid_for(n, 256), 256, 0, stream_>>>(x_.ptr, n, pt_bounds_.ptr, pt_code_.ptr, pt_ids_.ptr);
+    CC_CUDA(cudaGetLastError());
+    return 3 + sorter_.sort_pairs(pt_code_.ptr, pt_code_s_.ptr, pt_ids_.ptr, point_order_.ptr, n, 63, stream_,
+                                  &stats_d_.ptr->error, DERR_SORT_WAIT);
+}
+
 void World::build_candidates(double R, double skin) {
     double search = R + 2.0 * skin + 1e-12;  // candidates.rs:23-28
     double search2 = search * search;
-    launches_ += tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_, &stats_d_.ptr->error);
-    launches_ += tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_, &stats_d_.ptr->error);
-    LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
-    LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
+    launches_ += update_trees();
+    LbvhView tm = tree_tri_moving_.view(), tf = tree_tri_fixed_.view();
+    LbvhView em = tree_edge_moving_.view(), ef = tree_edge_fixed_.view();
+    const uint32_t* edges_in_leaf_order = tree_edge_moving_.leaf_prim.ptr;
     if (vf_cap_ == 0) {
         // generous first capacities: the in-plane pairs of a sheet at the
         // candidate radius alone reach ~60 per edge
@@ -1078,15 +1299,24 @@ void World::build_candidates(double R, double skin) {
     for (int attempt = 0; attempt < 8; ++attempt) {
         vf_.reserve(vf_cap_);
         ee_.reserve(ee_cap_);
-        CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_vf, 0, sizeof(unsigned long long), stream_));
+        // the VF query on the side stream (after its tree), the EE query on
+        // the main one: the VF query's one thread per point leaves most of the
+        // GPU to the EE query
+        // (the side stream also waits for the point order, made on the main
+        // stream when the trees are built)
+        CC_CUDA(cudaEventRecord(fork_, stream_));
+        CC_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
+        CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_vf, 0, sizeof(unsigned long long), side_));
         CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_ee, 0, sizeof(unsigned long long), stream_));
-        k_vf_query<<<grid_for(n_all_, 128), 128, 0, stream_>>>(view(), tm, tf, search2, vf_.ptr, vf_cap_,
-                                                                &stats_d_.ptr->n_vf, &stats_d_.ptr->error);
+        k_vf_query<<<grid_for(n_all_, 128), 128, 0, side_>>>(view(), point_order_.ptr, tm, tf, search2, vf_.ptr,
+                                                              vf_cap_, &stats_d_.ptr->n_vf, &stats_d_.ptr->error);
         k_ee_query<<<grid_for(edge_moving_h_.size(), 128), 128, 0, stream_>>>(
-            view(), edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), em, ef, search2, ee_.ptr, ee_cap_,
+            view(), edges_in_leaf_order, (uint32_t)edge_moving_h_.size(), em, ef, search2, ee_.ptr, ee_cap_,
             &stats_d_.ptr->n_ee, &stats_d_.ptr->error);
         launches_ += 2;
         CC_CUDA(cudaGetLastError());
+        CC_CUDA(cudaEventRecord(join_, side_));
+        CC_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
         sync_stats();
         raise_device_error(stats_h_.ptr->error);
         bool grow = false;
@@ -1160,24 +1390,17 @@ void World::detect(double query_radius, double radius, double relaxation, double
     }
     mark(2);
     unsigned long long n_vf = stats_h_.ptr->n_vf, n_ee = stats_h_.ptr->n_ee;
-    // bits per vertex id in the contact keys: the radix sorts below run only
-    // over the 2nb + 2 (hi) and 2nb (lo) bits the keys use
-    uint32_t nb = 1;
-    while ((1ull << nb) < (unsigned long long)n_all_) ++nb;
     // narrow phase
     if (raw_cap_ == 0) raw_cap_ = std::max<size_t>(4096, (size_t)(n_vf + n_ee) / 2 + 4096);
     for (int attempt = 0; attempt < 8; ++attempt) {
-        raw_hi_.reserve(raw_cap_);
-        raw_lo_.reserve(raw_cap_);
-        raw_eps_.reserve(raw_cap_);
-        raw_idx_.reserve(raw_cap_);
+        raw_key_.reserve(raw_cap_);
         CC_CUDA(cudaMemsetAsync(&sd->n_raw, 0, sizeof(unsigned long long), stream_));
         CC_CUDA(cudaMemsetAsync(&sd->vf_count, 0, sizeof(unsigned long long) * 3, stream_));
         unsigned long long qbits;
         std::memcpy(&qbits, &query_radius, 8);
         k_fill_u64<<<grid_for(n_all_, 256), 256, 0, stream_>>>(dist_bits_.ptr, n_all_, qbits);
-        NarrowOut o{raw_hi_.ptr,   raw_lo_.ptr,    raw_eps_.ptr,   raw_idx_.ptr,      raw_cap_, &sd->n_raw,
-                    dist_bits_.ptr, &sd->vf_count, &sd->ee_count, &sd->rejections, nb};
+        NarrowOut o{raw_key_.ptr,    raw_cap_,           &sd->n_raw,        dist_bits_.ptr, &sd->vf_count,
+                    &sd->ee_count,   &sd->rejections,    edge_rank_.ptr,    tri_rank_.ptr,  key_bits_};
         unsigned long long total = n_vf + n_ee;
         k_narrow<<<grid_for((size_t)total, 128), 128, 0, stream_>>>(view(), vf_.ptr, n_vf, ee_.ptr, n_ee, query_radius,
                                                                     &sd->max_abs_bits, prune ? 1 : 0, o);
@@ -1187,43 +1410,31 @@ void World::detect(double query_radius, double radius, double relaxation, double
         sync_stats();
         if (stats_h_.ptr->n_raw <= raw_cap_) break;
         raw_cap_ = (size_t)(stats_h_.ptr->n_raw * 1.5) + 4096;
-        raw_hi_.release();
-        raw_lo_.release();
-        raw_eps_.release();
-        raw_idx_.release();
+        raw_key_.release();
     }
     size_t n_raw = stats_h_.ptr->n_raw;
     if (n_raw > raw_cap_) throw Failure{CC_ERR_CUDA, "OGC contact buffer could not be sized"};
-    // canonical order: stable LSD radix sort on (lo) then (hi). The unique
-    // count stays on the device (sd->n_contacts): the kernels below read it and
-    // their grids and buffers are sized for n_raw, so the host learns it only at
-    // the detection's final read-back.
+    // canonical order: one keys-only radix sort over the 2W + 2 bits the keys
+    // use, then dedup. The unique count stays on the device (sd->n_contacts):
+    // the kernels below read it and their grids and buffers are sized for
+    // n_raw, so the host learns it only at the detection's final read-back.
     if (n_raw > 0) {
-        raw_hi_s_.reserve(n_raw);
-        raw_lo_s_.reserve(n_raw);
-        raw_idx_s_.reserve(n_raw);
+        raw_key_s_.reserve(n_raw);
         uniq_flag_.reserve(n_raw);
         uniq_pos_.reserve(n_raw);
-        const int lo_bits = (int)(2 * nb), hi_bits = (int)(2 * nb + 2);
-        launches_ += sorter_.sort_pairs(raw_lo_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_idx_s_.ptr, n_raw, lo_bits,
-                                        stream_, &sd->error, DERR_SORT_WAIT);
-        // gather hi in lo order, then stable sort by hi
-        k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_idx_s_.ptr, raw_hi_s_.ptr, n_raw);
-        launches_ += sorter_.sort_pairs(raw_hi_s_.ptr, raw_hi_.ptr, raw_idx_s_.ptr, raw_idx_.ptr, n_raw, hi_bits,
-                                        stream_, &sd->error, DERR_SORT_WAIT);
-        // raw_hi_ = sorted hi, raw_idx_ = original index; gather lo
-        k_gather_u64<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_lo_.ptr, raw_idx_.ptr, raw_lo_s_.ptr, n_raw);
-        k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, n_raw, uniq_flag_.ptr);
+        launches_ += sorter_.sort_keys(raw_key_.ptr, raw_key_s_.ptr, n_raw, (int)(2 * key_bits_ + 2), stream_,
+                                       &sd->error, DERR_SORT_WAIT);
+        k_unique_flags<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_key_s_.ptr, n_raw, uniq_flag_.ptr);
         launches_ += exclusive_sum(uniq_flag_.ptr, uniq_pos_.ptr, n_raw, scan_tmp_, stream_);
         k_unique_count<<<1, 1, 0, stream_>>>(uniq_flag_.ptr, uniq_pos_.ptr, n_raw, &sd->n_contacts);
-        ++launches_;
         c_kind_.reserve(n_raw);
         c_verts_.reserve(n_raw);
         c_eps_.reserve(n_raw);
-        k_compact<<<grid_for(n_raw, 256), 256, 0, stream_>>>(raw_hi_.ptr, raw_lo_s_.ptr, raw_idx_.ptr, raw_eps_.ptr,
-                                                             uniq_flag_.ptr, uniq_pos_.ptr, n_raw, c_kind_.ptr,
-                                                             c_verts_.ptr, c_eps_.ptr, nb);
-        launches_ += 4;
+        RankTables rt{rank_edge_verts_.ptr, rank_edge_id_.ptr, rank_tri_verts_.ptr};
+        k_compact<<<grid_for(n_raw, 256), 256, 0, stream_>>>(view(), raw_key_s_.ptr, uniq_flag_.ptr, uniq_pos_.ptr,
+                                                             n_raw, rt, key_bits_, c_kind_.ptr, c_verts_.ptr,
+                                                             c_eps_.ptr);
+        launches_ += 3;
     }
     // incidence (moving vertices), active count, radii
     CC_CUDA(cudaMemsetAsync(inc_count_.ptr, 0, (moving_ + 1) * sizeof(uint32_t), stream_));
@@ -1271,9 +1482,11 @@ void World::validate_start() {  // world.rs:242-307
     unsigned long long none = ~0ull;
     CC_CUDA(cudaMemcpyAsync(&stats_d_.ptr->intersect_key, &none, 8, cudaMemcpyHostToDevice, stream_));
     refit(true);
-    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_, &stats_d_.ptr->error);
-    k_intersections<<<grid_for(n_tri_, 128), 128, 0, stream_>>>(view(), tree_tri_moving_.view(tri_box_.ptr),
-                                                                tree_tri_fixed_.view(tri_box_.ptr), nullptr,
+    launches_ += update_trees();
+    CC_CUDA(cudaEventRecord(join_, side_));
+    CC_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
+    k_intersections<<<grid_for(n_tri_, 128), 128, 0, stream_>>>(view(), tree_tri_moving_.view(),
+                                                                tree_tri_fixed_.view(), nullptr,
                                                                 &stats_d_.ptr->intersect_key, &stats_d_.ptr->error);
     CC_CUDA(cudaGetLastError());
     sync_stats();
@@ -1307,25 +1520,30 @@ void World::fresh_pairs(double search, std::vector<uint32_t>& vf, std::vector<ui
     // exact search radius: build_candidates adds 2*skin + 1e-12, so pass R
     // such that the sum equals `search`
     double search2 = search * search;
-    tree_tri_moving_.build(tri_box_.ptr, tri_moving_.ptr, (uint32_t)tri_moving_h_.size(), stream_, &stats_d_.ptr->error);
-    tree_edge_moving_.build(edge_box_.ptr, edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), stream_, &stats_d_.ptr->error);
-    LbvhView tm = tree_tri_moving_.view(tri_box_.ptr), tf = tree_tri_fixed_.view(tri_box_.ptr);
-    LbvhView em = tree_edge_moving_.view(edge_box_.ptr), ef = tree_edge_fixed_.view(edge_box_.ptr);
+    launches_ += update_trees();
+    CC_CUDA(cudaEventRecord(join_, side_));
+    CC_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
+    LbvhView tm = tree_tri_moving_.view(), tf = tree_tri_fixed_.view();
+    LbvhView em = tree_edge_moving_.view(), ef = tree_edge_fixed_.view();
     size_t vcap = std::max<size_t>(1024, 16 * n_all_), ecap = std::max<size_t>(1024, 32 * n_edge_);
     for (int attempt = 0; attempt < 8; ++attempt) {
         DBuf<uint2> a, b;
         a.reserve(vcap);
         b.reserve(ecap);
-        CC_CUDA(cudaMemsetAsync(&stats_d_.ptr->n_vf, 0, 16, stream_));
-        k_vf_query<<<grid_for(n_all_, 128), 128, 0, stream_>>>(view(), tm, tf, search2, a.ptr, vcap,
-                                                                &stats_d_.ptr->n_vf, &stats_d_.ptr->error);
+        // own counters: n_vf / n_ee in the stats belong to the candidate cache
+        fresh_counts_.reserve(2);
+        CC_CUDA(cudaMemsetAsync(fresh_counts_.ptr, 0, 2 * sizeof(unsigned long long), stream_));
+        k_vf_query<<<grid_for(n_all_, 128), 128, 0, stream_>>>(view(), point_order_.ptr, tm, tf, search2, a.ptr,
+                                                                vcap, fresh_counts_.ptr, &stats_d_.ptr->error);
         k_ee_query<<<grid_for(edge_moving_h_.size(), 128), 128, 0, stream_>>>(
-            view(), edge_moving_.ptr, (uint32_t)edge_moving_h_.size(), em, ef, search2, b.ptr, ecap,
-            &stats_d_.ptr->n_ee, &stats_d_.ptr->error);
+            view(), tree_edge_moving_.leaf_prim.ptr, (uint32_t)edge_moving_h_.size(), em, ef, search2, b.ptr, ecap,
+            fresh_counts_.ptr + 1, &stats_d_.ptr->error);
         CC_CUDA(cudaGetLastError());
+        unsigned long long counts[2];
+        CC_CUDA(cudaMemcpyAsync(counts, fresh_counts_.ptr, sizeof counts, cudaMemcpyDeviceToHost, stream_));
         sync_stats();
         raise_device_error(stats_h_.ptr->error);
-        size_t nv = stats_h_.ptr->n_vf, ne = stats_h_.ptr->n_ee;
+        size_t nv = counts[0], ne = counts[1];
         if (nv > vcap || ne > ecap) {
             vcap = std::max(vcap, nv + 1);
             ecap = std::max(ecap, ne + 1);
@@ -1343,7 +1561,6 @@ void World::fresh_pairs(double search, std::vector<uint32_t>& vf, std::vector<ui
         ee.clear();
         for (auto& p : sv) vf.insert(vf.end(), p.begin(), p.end());
         for (auto& p : se) ee.insert(ee.end(), p.begin(), p.end());
-        cache_valid_ = false;  // the cache buffers were not touched, but the trees were
         return;
     }
     throw Failure{CC_ERR_CUDA, "OGC candidate buffers could not be sized"};

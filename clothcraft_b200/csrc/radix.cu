@@ -1,5 +1,6 @@
 // Stable LSD radix sort and prefix sums (see radix.cuh).
 #include <algorithm>
+#include <type_traits>
 
 #include "radix.cuh"
 
@@ -192,7 +193,7 @@ __global__ void __launch_bounds__(kBlock) k_onesweep_pass(const K* __restrict__ 
         if (i < n) {
             uint32_t pos = goff[dig[j]] + rank[j];
             kout[pos] = key[j];
-            vout[pos] = vin[i];
+            if constexpr (!std::is_same<V, NoValue>::value) vout[pos] = vin[i];
         }
     }
 }
@@ -251,12 +252,13 @@ int prefix_sum(const T* in, T* out, size_t n, DBuf<T>& scratch, cudaStream_t s) 
 }  // namespace
 
 template <class K, class V>
-int RadixSorter::sort_pairs(const K* keys_in, K* keys_out, const V* vals_in, V* vals_out, size_t n, int bits,
-                            cudaStream_t s, unsigned int* err, unsigned int err_bit) {
+int RadixSorter::sort_impl(const K* keys_in, K* keys_out, const V* vals_in, V* vals_out, size_t n, int bits,
+                           cudaStream_t s, unsigned int* err, unsigned int err_bit) {
+    constexpr bool kVals = !std::is_same<V, NoValue>::value;
     if (n == 0) return 0;
     if (bits <= 0) {
         CC_CUDA(cudaMemcpyAsync(keys_out, keys_in, n * sizeof(K), cudaMemcpyDeviceToDevice, s));
-        CC_CUDA(cudaMemcpyAsync(vals_out, vals_in, n * sizeof(V), cudaMemcpyDeviceToDevice, s));
+        if constexpr (kVals) CC_CUDA(cudaMemcpyAsync(vals_out, vals_in, n * sizeof(V), cudaMemcpyDeviceToDevice, s));
         return 0;
     }
     if (n > kCountMask) throw Failure{CC_ERR_INVALID_ARGUMENT, "radix sort: more than 2^30 keys"};
@@ -276,9 +278,11 @@ int RadixSorter::sort_pairs(const K* keys_in, K* keys_out, const V* vals_in, V* 
     V* vtmp = nullptr;
     if (passes > 1) {
         keys_tmp_.reserve(n * sizeof(K));
-        vals_tmp_.reserve(n * sizeof(V));
         ktmp = reinterpret_cast<K*>(keys_tmp_.ptr);
-        vtmp = reinterpret_cast<V*>(vals_tmp_.ptr);
+        if constexpr (kVals) {
+            vals_tmp_.reserve(n * sizeof(V));
+            vtmp = reinterpret_cast<V*>(vals_tmp_.ptr);
+        }
     }
     unsigned hist_grid = (unsigned)std::min<size_t>(tiles, 148 * 4);
     k_onesweep_hist<K><<<hist_grid, kBlock, 0, s>>>(keys_in, n, passes, bits, offs);
@@ -302,6 +306,18 @@ int RadixSorter::sort_pairs(const K* keys_in, K* keys_out, const V* vals_in, V* 
     return 2 + passes;
 }
 
+template <class K, class V>
+int RadixSorter::sort_pairs(const K* keys_in, K* keys_out, const V* vals_in, V* vals_out, size_t n, int bits,
+                            cudaStream_t s, unsigned int* err, unsigned int err_bit) {
+    return sort_impl<K, V>(keys_in, keys_out, vals_in, vals_out, n, bits, s, err, err_bit);
+}
+
+template <class K>
+int RadixSorter::sort_keys(const K* keys_in, K* keys_out, size_t n, int bits, cudaStream_t s, unsigned int* err,
+                           unsigned int err_bit) {
+    return sort_impl<K, NoValue>(keys_in, keys_out, nullptr, nullptr, n, bits, s, err, err_bit);
+}
+
 template int RadixSorter::sort_pairs<uint16_t, uint32_t>(const uint16_t*, uint16_t*, const uint32_t*, uint32_t*,
                                                           size_t, int, cudaStream_t, unsigned int*, unsigned int);
 template int RadixSorter::sort_pairs<unsigned long long, uint32_t>(const unsigned long long*, unsigned long long*,
@@ -310,6 +326,8 @@ template int RadixSorter::sort_pairs<unsigned long long, uint32_t>(const unsigne
 template int RadixSorter::sort_pairs<unsigned long long, double>(const unsigned long long*, unsigned long long*,
                                                                   const double*, double*, size_t, int, cudaStream_t,
                                                                   unsigned int*, unsigned int);
+template int RadixSorter::sort_keys<unsigned long long>(const unsigned long long*, unsigned long long*, size_t, int,
+                                                         cudaStream_t, unsigned int*, unsigned int);
 
 template <class T>
 int exclusive_sum(const T* in, T* out, size_t n, DBuf<T>& scratch, cudaStream_t s) {

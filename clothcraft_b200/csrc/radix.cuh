@@ -17,6 +17,8 @@
 
 namespace cc {
 
+struct NoValue {};  // the value type of a keys-only sort
+
 class RadixSorter {
    public:
     // keys_out/vals_out[i] = the pairs of keys_in/vals_in ordered by the low
@@ -26,8 +28,15 @@ class RadixSorter {
     template <class K, class V>
     int sort_pairs(const K* keys_in, K* keys_out, const V* vals_in, V* vals_out, size_t n, int bits,
                    cudaStream_t s, unsigned int* err = nullptr, unsigned int err_bit = 1u);
+    // The same for keys alone (K: uint64_t).
+    template <class K>
+    int sort_keys(const K* keys_in, K* keys_out, size_t n, int bits, cudaStream_t s, unsigned int* err = nullptr,
+                  unsigned int err_bit = 1u);
 
    private:
+    template <class K, class V>
+    int sort_impl(const K* keys_in, K* keys_out, const V* vals_in, V* vals_out, size_t n, int bits, cudaStream_t s,
+                  unsigned int* err, unsigned int err_bit);
     DBuf<uint32_t> hist_;
     DBuf<unsigned int> err_;
     DBuf<unsigned char> keys_tmp_, vals_tmp_;

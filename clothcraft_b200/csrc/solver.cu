@@ -1661,6 +1661,13 @@ void cc_world_destroy(cc_world* w) {
     if (w && w->own) delete w;
 }
 
+int32_t cc_world_set_tree_rebuild_period(cc_world* w, int32_t period) {
+    if (!w) return CC_ERR_INVALID_ARGUMENT;
+    if (period < 0) return w->fail(Failure{CC_ERR_INVALID_ARGUMENT, "tree rebuild period must be >= 0"});
+    w->w->set_tree_rebuild_period((uint32_t)period);
+    return CC_OK;
+}
+
 int32_t cc_world_validate_start(cc_world* w, const double* x) {
     try {
         Pinned<double4> stage;

@@ -14,32 +14,47 @@ struct Box {
     double hi[3];
 };
 
-// Karras LBVH over a subset of primitives (ids) with boxes in a global array.
-struct LbvhView {
-    uint32_t m;               // leaves
-    const Box* node_box;      // [m-1] internal boxes
-    const int2* child;        // [m-1] children; bit 31 set = leaf (sorted position)
-    const uint32_t* leaf_prim;  // [m] primitive id of each sorted leaf
-    const Box* prim_box;      // global primitive boxes, indexed by primitive id
-    const uint32_t* node_max;  // [m-1] largest primitive id under each internal node
+// One internal LBVH node as a traversal reads it: both children's boxes,
+// rounded outward to FP32 (lo down, hi up, so each contains the exact FP64
+// box of everything below it), the children's indices and the largest
+// primitive id below each child, in one 64-byte record. A visit is one
+// record read; only the leaves are tested against their exact FP64 boxes.
+//   a = left lo.xyz, left hi.x     b = left hi.yz, right lo.xy
+//   c = right lo.z, right hi.xyz   d = left child, right child (bit 31 set:
+//   a leaf, by sorted position), largest id below left, below right
+struct alignas(16) LNode {
+    float4 a, b, c;
+    int4 d;
 };
 
+// Karras LBVH over a subset of primitives (ids) with boxes in a global array.
+struct LbvhView {
+    uint32_t m;                 // leaves
+    const LNode* node;          // [m-1] internal nodes, root 0
+    const uint32_t* leaf_prim;  // [m] primitive id of each sorted leaf
+    const Box* leaf_box;        // [m] exact primitive boxes in leaf order
+};
+
+// The topology (Morton order, Karras split) comes from build(); refit()
+// recomputes the boxes for the current primitive boxes and keeps the
+// topology, as the reference's Bvh keeps its tree and refits it
+// (src/ogc/bvh.rs). Either way every primitive box is inside its ancestors'
+// boxes, so a traversal finds the same pair set.
 struct Lbvh {
     uint32_t m = 0;
-    DBuf<Box> node_box;
-    DBuf<uint32_t> node_max;
-    DBuf<int2> child;
+    bool built = false;
+    DBuf<LNode> node;       // [m-1]
     DBuf<int> parent;       // [2m-1]: internal 0..m-2, leaves m-1..2m-2
     DBuf<unsigned> visits;  // [m-1]
     DBuf<uint32_t> leaf_prim, ids_tmp;
+    DBuf<Box> leaf_box;     // [m]
     DBuf<unsigned long long> morton, morton_tmp;
     DBuf<unsigned long long> bounds;  // 6 order keys
     RadixSorter sorter;
-    // returns the number of this library's kernels launched
+    // Both return the number of this library's kernels launched.
     int build(const Box* prim_box, const uint32_t* ids, uint32_t m, cudaStream_t s, unsigned int* err);
-    LbvhView view(const Box* prim_box) const {
-        return {m, node_box.ptr, child.ptr, leaf_prim.ptr, prim_box, node_max.ptr};
-    }
+    int refit(const Box* prim_box, cudaStream_t s);  // after a build over the same primitives
+    LbvhView view() const { return {m, node.ptr, leaf_prim.ptr, leaf_box.ptr}; }
 };
 
 // Static topology (src/ogc/topology.rs:13-52), built on the host at creation.
@@ -132,14 +147,28 @@ class World {
     };
     void set_profiling(bool on) { profile_ = on; }
     const PhaseMs& last_phase_ms() const { return phase_ms_; }
+    // LBVH topology policy for the moving trees at a candidate rebuild: 0 =
+    // keep the topology of the first build and refit it (the reference's
+    // tree), k >= 1 = rebuild it from Morton codes every k-th candidate
+    // rebuild and refit in between.
+    void set_tree_rebuild_period(uint32_t k) { tree_period_ = k; }
+    uint32_t tree_rebuild_period() const { return tree_period_; }
+    uint64_t tree_builds() const { return tree_builds_; }
 
    private:
     WorldView view() const;
     void refit(bool check_fixed);
     void build_candidates(double R, double skin);
+    int update_trees();  // moving trees for the current boxes, on two streams
+    int order_points();  // point_order_ from the current positions
     void sync_stats();
 
     cudaStream_t stream_;
+    cudaStream_t side_ = nullptr;  // second stream for the triangle side of a rebuild
+    cudaEvent_t fork_ = nullptr, join_ = nullptr;
+    uint32_t tree_period_ = 0;
+    uint32_t rebuilds_since_build_ = 0;
+    uint64_t tree_builds_ = 0;
     size_t n_all_, moving_, n_tri_, n_edge_;
     TopologyHost top_;
     std::vector<uint32_t> tri_moving_h_, tri_fixed_h_, edge_moving_h_, edge_fixed_h_;
@@ -160,11 +189,17 @@ class World {
     DBuf<double4> cache_centers_;
     DBuf<uint2> vf_, ee_;
     size_t vf_cap_ = 0, ee_cap_ = 0;
+    DBuf<unsigned long long> fresh_counts_;  // fresh_pairs' own pair counts
+    DBuf<uint32_t> point_order_, pt_ids_;     // VF query order (Morton order of all points)
+    DBuf<unsigned long long> pt_code_, pt_code_s_, pt_bounds_;
 
     // narrow phase + canonical set
-    DBuf<unsigned long long> raw_hi_, raw_lo_, raw_hi_s_, raw_lo_s_;
-    DBuf<double> raw_eps_;
-    DBuf<uint32_t> raw_idx_, raw_idx_s_, uniq_flag_, uniq_pos_;
+    DBuf<unsigned long long> raw_key_, raw_key_s_;  // packed contact keys (detect.cu)
+    DBuf<uint32_t> uniq_flag_, uniq_pos_;
+    DBuf<uint32_t> edge_rank_, tri_rank_, rank_edge_id_;  // contact-key ranks
+    DBuf<uint2> rank_edge_verts_;
+    DBuf<uint3> rank_tri_verts_;
+    uint32_t key_bits_ = 1;
     size_t raw_cap_ = 0;
     DBuf<uint32_t> c_kind_;
     DBuf<uint4> c_verts_;

@@ -57,6 +57,7 @@ SIGNATURES = {
                                     C.POINTER(cc_contacts)]),
     "cc_world_candidates": (C.c_int32, [C.c_void_p, c_double_p, C.c_double, C.POINTER(cc_candidates)]),
     "cc_world_edges": (C.c_uint64, [C.c_void_p, c_uint32_p]),
+    "cc_world_set_tree_rebuild_period": (C.c_int32, [C.c_void_p, C.c_int32]),
     "cc_batch_create": (C.c_int32, [C.POINTER(cc_mesh), C.POINTER(cc_surface), C.POINTER(c_double_p),
                                     C.POINTER(c_double_p), C.c_uint64, C.POINTER(C.c_void_p)]),
     "cc_batch_instances": (C.c_uint64, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_uint64]),

@@ -35,6 +35,8 @@ def main(argv=None):
     ap.add_argument("--lanes32", type=int, default=8 | 4 << 8)
     ap.add_argument("--profile", action="store_true", help="time each iteration's sweeps with CUDA events")
     ap.add_argument("--graphs", action="store_true", help="launch the iteration chunks as CUDA graphs")
+    ap.add_argument("--tree-period", type=int, default=None,
+                    help="LBVH rebuild period at candidate rebuilds (0: refit the first build's trees)")
     args = ap.parse_args(argv)
     sc = scenes.config1()
     z = np.load(FOLD_STATE)
@@ -54,6 +56,8 @@ def main(argv=None):
     g.set_state(z["x"].astype(np.float64), z["v"].astype(np.float64), float(z["time"]))
     g.set_profiling(args.profile)
     g.set_graphs(args.graphs)
+    if args.tree_period is not None:
+        g.world.set_tree_rebuild_period(args.tree_period)
     for k in range(args.steps):
         m = g.step_resident(s.to_c())
         print("step %d: %d iterations, %.2f ms, residual %s, sweeps %.3f ms in %d launches, detection %.3f ms "

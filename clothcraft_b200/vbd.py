@@ -121,6 +121,13 @@ class OgcWorld:
                 raise self._err(rc)
             return vf[:out.n_vf].copy(), ee[:out.n_ee].copy()
 
+    def set_tree_rebuild_period(self, period: int):
+        """LBVH policy at a candidate rebuild: 0 refits the first build's
+        trees (the reference's tree), k >= 1 rebuilds them every k-th time."""
+        rc = native.load().cc_world_set_tree_rebuild_period(self.h, int(period))
+        if rc != 0:
+            raise self._err(rc)
+
     def edges(self):
         L = native.load()
         n = L.cc_world_edges(self.h, None)

@@ -389,6 +389,15 @@ int32_t cc_world_candidates(cc_world* world, const double* x, double radius,
                             cc_candidates* out);
 /* Topology sizes: edges of the combined mesh (src/ogc/topology.rs:13-52). */
 uint64_t cc_world_edges(const cc_world* world, uint32_t* edges_out);
+/* LBVH policy of the moving triangle and edge trees at a candidate rebuild:
+ * 0 (the default) builds each tree once, from the Morton codes of the first
+ * rebuild's boxes, and refits it at every later rebuild, as the reference
+ * keeps its median-split tree and refits it (src/ogc/bvh.rs:66-242);
+ * k >= 1 builds the trees again at every k-th rebuild and refits in between.
+ * The candidate pair sets do not depend on it (every primitive's box is
+ * inside its ancestors' boxes whatever the topology); only the traversal
+ * cost does. For a solver, pass cc_solver_world(solver). */
+int32_t cc_world_set_tree_rebuild_period(cc_world* world, int32_t period);
 
 /* -------------------------------------------------- batched instances */
 /* Many independent cloths stepped as one solver (no reference counterpart;
