@@ -184,3 +184,35 @@ def test_random_displacements_against_oracle():
         x[:n] += rng.uniform(-1e-3, 1e-3, (n, 3))
         a, b = g.detect(x, 0.008, ogc(0.002)), o.detect(x, 0.008, ogc(0.002))
         assert_same_contacts(a, b, k)
+
+
+def test_tree_rebuild_period_does_not_change_detections():
+    """The LBVH policy (refit the first build's trees, or rebuild them every
+    k-th candidate rebuild) changes only the traversal cost: worlds created on
+    the flat sheet and detected while it folds into layers give the oracle's
+    contact sets and candidate lists for every period."""
+    sc = scenes.small_sheet(24, seed=3, radius=0.002, side=0.3, height=0.12)
+    obs = sc.obstacle
+    n = sc.n
+    _, xf = folded_sheet(24, 3)
+    flat = np.concatenate([sc.x0, obs.vertices])
+    tris = np.concatenate([sc.mesh.triangles, obs.triangles + n])
+    worlds = []
+    for period in (0, 1, 3):
+        w = OgcWorld(flat, tris, n)
+        w.set_tree_rebuild_period(period)
+        worlds.append(w)
+    o = oracle.World(flat, tris, n)
+    with pytest.raises(VbdError):
+        worlds[0].set_tree_rebuild_period(-1)
+    for frame in range(8):
+        s = frame / 7.0
+        x = flat.copy()
+        x[:n] = (1.0 - s) * sc.x0 + s * xf
+        ref = o.detect(x, 0.004, ogc(0.002))
+        for w in worlds:
+            assert_same_contacts(w.detect(x, 0.004, ogc(0.002)), ref, frame)
+    vf_o, ee_o = o.candidates(x, 0.0101)
+    for w in worlds:
+        vf_g, ee_g = w.candidates(x, 0.0101)
+        assert np.array_equal(vf_g, vf_o) and np.array_equal(ee_g, ee_o)
