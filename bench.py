@@ -419,7 +419,7 @@ def main():
     warm_state = learned.get_state()
     clocks = ClockSampler(local).__enter__()
     # ---- value: learned init at equal residual, device-resident; the colour
-    # sweeps of every iteration are bracketed by one event pair (the roofline's
+    # sweeps of every iteration stamp their span on the device clock (the roofline's
     # launch durations and the breakdown come from this same timed leg)
     L.cc_solver_set_profiling(learned.h, 1)
     t_l, mets_l = leg(learned, lambda: learned.step_resident(st_l), K)
@@ -427,11 +427,11 @@ def main():
     # ---- plain adaptive init at equal residual
     t_p, mets_p = leg(plain, lambda: plain.step_resident(st_p), K)
     # ---- the value leg's settings with every kernel launched directly (no CUDA
-    # graphs) and without the per-iteration sweep events
+    # graphs) and without the per-iteration sweep stamps
     direct_solver = make(1)
     direct_solver.set_graphs(False)
     t_g, mets_g = leg(direct_solver, lambda: direct_solver.step_resident(st_l), K)
-    # ---- the value leg's settings, CUDA graphs, without the sweep events
+    # ---- the value leg's settings, CUDA graphs, without the sweep stamps or detection phase events
     quiet_solver = make(1)
     t_q, mets_q = leg(quiet_solver, lambda: quiet_solver.step_resident(st_l), K)
     # ---- both inits at the other sweep precision (same target and acceleration)
@@ -512,7 +512,8 @@ def main():
                  "sweeps": sweep_ms / K,
                  "other": t_l / K - det_ms - col_ms - init_ms - sweep_ms / K,
                  "note": "from the timed learned leg: detection and colouring by host clock (they end in a "
-                         "device sync), learned guess and sweeps by CUDA events; detection_device = the "
+                         "device sync), learned guess by CUDA events, sweeps by the sweep kernels' device-clock "
+                         "stamps; detection_device = the "
                          "detection phases by CUDA events (refit and cache check, candidate rebuilds, narrow "
                          "phase with the canonical sort, incidence and radii); other = ms_per_step minus "
                          "detection, colouring, learned guess and sweeps (predict, warm start, residual "
@@ -560,12 +561,13 @@ def main():
         "learned_init_used_fraction": float(np.mean([m["init_used"] for m in mets_l])),
         "acceleration": ACCELERATION,
         "launch_forms": {
-            "graphs_with_sweep_events": {"steps_per_s": world * K / (t_l / 1000.0), "ms_per_step": t_l / K},
+            "graphs_with_sweep_stamps": {"steps_per_s": world * K / (t_l / 1000.0), "ms_per_step": t_l / K},
             "graphs": {"steps_per_s": world * K / (t_q / 1000.0), "ms_per_step": t_q / K},
             "direct_launches": {"steps_per_s": world * K / (t_g / 1000.0), "ms_per_step": t_g / K},
-            "note": "the value leg (iteration chunks launched as CUDA graphs, per-iteration sweep events "
-                    "recorded by event nodes) against the same steps without the events, and with every "
-                    "kernel launched directly; identical iterates"},
+            "note": "the value leg (iteration chunks launched as CUDA graphs, the sweep kernels stamping "
+                    "their per-iteration span on the device clock, detection phases timed by CUDA events) "
+                    "against the same steps without any timing, and with every kernel launched directly; "
+                    "identical iterates"},
         "sweep_precision": ("fp32 element assembly" if SWEEP_PRECISION else "fp64"),
         "other_precision": {"sweep_precision": ("fp32 element assembly" if other else "fp64"),
                             "learned": summary(*other_legs[1]), "plain": summary(*other_legs[0]),
@@ -593,8 +595,9 @@ def main():
             "peak_kind": peak_kind,
             "sweep_launches": int(sweeps),
             "avg_launch_us": 1000.0 * sweep_ms / max(sweeps, 1),
-            "launch_timing": "CUDA events around each iteration's back-to-back colour sweeps in the timed "
-                             "learned leg, divided by the launches",
+            "launch_timing": "each iteration's back-to-back colour sweeps timed in the timed learned leg by "
+                             "their own device-clock stamps (first colour's earliest block start to the last "
+                             "colour's latest block end), summed and divided by the launches",
             "algorithmic_bytes_per_launch": alg_bytes / max(sweeps, 1),
             "sweep_share_of_step": sweep_ms / t_l,
         },

@@ -465,7 +465,10 @@ struct cc_solver {
     DBuf<double> ext_scan;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, tune0 = nullptr, tune1 = nullptr;
     bool profiling = false;
-    std::vector<cudaEvent_t> prof_events;
+    // profiling: per-iteration sweep-span stamps (ns, %globaltimer) written by the
+    // first and last colour's blocks; no event is recorded between the sweeps
+    DBuf<unsigned long long> stamp_s, stamp_e;
+    Pinned<unsigned long long> stamp_h;
     uint64_t own_launches = 0;
     uint32_t n_free = 0;
     int lanes = 0;          // vertices are solved by groups of `lanes` threads; 0 = autotune on next step
@@ -513,7 +516,6 @@ struct cc_solver {
             if (e) cudaEventDestroy(e);
         if (learn0) cudaEventDestroy(learn0);
         if (learn1) cudaEventDestroy(learn1);
-        for (auto e : prof_events) cudaEventDestroy(e);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -596,12 +598,6 @@ struct cc_solver {
     bool graphs = true;
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_instantiations = 0, graph_updates = 0;
-    // an event record that also times inside a captured graph (an external
-    // event node records the event each time the graph runs)
-    void record_event(cudaEvent_t e, bool captured) {
-        if (captured) CC_CUDA(cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal));
-        else CC_CUDA(cudaEventRecord(e, stream));
-    }
     void launch_captured_chunk() {
         cudaGraph_t g = nullptr;
         CC_CUDA(cudaStreamEndCapture(stream, &g));
@@ -811,7 +807,6 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     cc_metrics m;
     std::memset(&m, 0, sizeof m);
     uint64_t launches0 = own_launches + world->launches() + coloring.launches();
-    size_t prof_used = 0;
     m.dt_s = s.dt;
     m.iterations = s.iterations;
     CC_CUDA(cudaEventRecord(ev0, stream));
@@ -893,8 +888,11 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         acc_b.reserve(n);
     }
     bool need_refresh = clipped > 0 && (double)clipped >= threshold;
-    std::vector<std::pair<size_t, uint32_t>> prof_pairs;  // (event index, iteration)
-    std::vector<uint32_t> prof_ok;
+    if (profiling) {
+        stamp_s.reserve(s.iterations);
+        stamp_e.reserve(s.iterations);
+        stamp_h.reserve(2 * (size_t)s.iterations);
+    }
     uint32_t it0 = 0, executed = s.iterations;
     CC_CUDA(cudaMemsetAsync(&sc.ptr->converged_at, 0xff, sizeof(unsigned int), stream));
     if (checks) CC_CUDA(cudaMemsetAsync(sc.ptr->gx2_iter, 0xff, sizeof(sc.ptr->gx2_iter), stream));  // NaN: not evaluated
@@ -922,7 +920,20 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         CC_CUDA(cudaMemsetAsync(&sc.ptr->stop_at, 0xff, sizeof(unsigned int), stream));
         CC_CUDA(cudaMemsetAsync(&sc.ptr->clipped_iter[it0], 0, (s.iterations - it0) * sizeof(unsigned int), stream));
         const auto& off = coloring.offsets();
-        size_t batch_first_pair = prof_pairs.size();
+        if (profiling) {  // this batch's iterations are (re)timed from scratch
+            CC_CUDA(cudaMemsetAsync(stamp_s.ptr + it0, 0xff, (s.iterations - it0) * sizeof(unsigned long long), stream));
+            CC_CUDA(cudaMemsetAsync(stamp_e.ptr + it0, 0, (s.iterations - it0) * sizeof(unsigned long long), stream));
+        }
+        uint32_t first_color = 0, last_color = 0;
+        {
+            bool any = false;
+            for (uint32_t c = 0; c < coloring.n_colors(); ++c)
+                if (off[c + 1] > off[c]) {
+                    if (!any) first_color = c;
+                    last_color = c;
+                    any = true;
+                }
+        }
         const uint32_t chunk = target_on ? std::max<uint32_t>(check_every, 4) : s.iterations;
         uint32_t chunks = 0;
         // graph mode: each chunk's launches are captured into a CUDA graph; the
@@ -937,26 +948,18 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
             for (uint32_t it = c0; it < c1; ++it) {
                 sv.iteration = it;
                 sv.clipped = &sc.ptr->clipped_iter[it];
-                // profiling: one event pair around the iteration's back-to-back
-                // colour sweeps (nothing else is enqueued between them)
-                if (profiling) {
-                    while (prof_events.size() < prof_used + 2) {
-                        cudaEvent_t e;
-                        CC_CUDA(cudaEventCreate(&e));
-                        prof_events.push_back(e);
-                    }
-                    record_event(prof_events[prof_used], capture);
-                }
+                // profiling: the iteration's back-to-back colour sweeps stamp
+                // their span (first colour's earliest block start, last
+                // colour's latest block end)
+                sv.stamp_start = profiling ? stamp_s.ptr + it : nullptr;
+                sv.stamp_end = profiling ? stamp_e.ptr + it : nullptr;
                 for (uint32_t c = 0; c < coloring.n_colors(); ++c) {
                     uint32_t cnt = off[c + 1] - off[c];
                     if (cnt == 0) continue;
+                    sv.stamp_first = c == first_color ? 1u : 0u;
+                    sv.stamp_last = c == last_color ? 1u : 0u;
                     sweep(sv, coloring.order() + off[c], cnt, fp32);
                     ++own_launches;
-                }
-                if (profiling) {
-                    record_event(prof_events[prof_used + 1], capture);
-                    prof_pairs.push_back({prof_used, it});
-                    prof_used += 2;
                 }
                 k_refresh_rule<<<1, 1, 0, stream>>>(sc.ptr, it, s.iterations, threshold, rho2);
                 if (accelerate) {
@@ -999,7 +1002,6 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         uint32_t ra = sc_h.ptr->refresh_at, ca = sc_h.ptr->converged_at;
         uint32_t done_to = std::min(std::min(ra, ca), s.iterations);
         m.sweep_launches += (uint64_t)(done_to - it0) * coloring.n_colors();
-        for (size_t k = batch_first_pair; k < prof_pairs.size(); ++k) prof_ok.push_back(prof_pairs[k].second < done_to);
         if (ca <= s.iterations && ca <= ra) {
             executed = ca;
             break;
@@ -1094,13 +1096,18 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
     m.extension_max_percent = metric_sort_failed ? std::nan("") : emax;
     m.detection_ms = det_ms;
     m.gpu_compute_ms = gms;
-    if (profiling) {
+    if (profiling && executed > 0) {
+        // iterations skipped after a refresh or a stop never stamp: their
+        // slots keep the empty values and are left out
+        CC_CUDA(cudaMemcpyAsync(stamp_h.ptr, stamp_s.ptr, executed * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaMemcpyAsync(stamp_h.ptr + executed, stamp_e.ptr, executed * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, stream));
+        CC_CUDA(cudaStreamSynchronize(stream));
         double sw = 0.0;
-        for (size_t k = 0; k < prof_pairs.size(); ++k) {
-            if (!prof_ok[k]) continue;  // enqueued past a refresh and skipped
-            float t = 0.f;
-            CC_CUDA(cudaEventElapsedTime(&t, prof_events[prof_pairs[k].first], prof_events[prof_pairs[k].first + 1]));
-            sw += t;
+        for (uint32_t it = 0; it < executed; ++it) {
+            unsigned long long a = stamp_h.ptr[it], b = stamp_h.ptr[executed + it];
+            if (a != ~0ull && b >= a) sw += (double)(b - a) * 1e-6;
         }
         m.sweep_ms = sw;
     }

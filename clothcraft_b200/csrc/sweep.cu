@@ -97,9 +97,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_sweep(SweepView s, const uint32
     const uint32_t lane = threadIdx.x & (G - 1);
     const unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
     constexpr uint32_t kGroups = BLOCK / G;
+    stamp_block_start(s);
     // whole groups step together
     for (uint32_t gi = blockIdx.x * kGroups + threadIdx.x / G; gi < count; gi += gridDim.x * kGroups)
         solve_vertex<G>(s, order[gi], lane, mask);
+    stamp_block_end(s);
 }
 
 template <int G, int B, int MINB>

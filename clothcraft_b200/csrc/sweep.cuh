@@ -53,7 +53,30 @@ struct SweepView {
     const unsigned int* skip_at;  // sweeps of iterations >= *skip_at exit at once (null: never)
     uint32_t iteration;
     unsigned char* clipped_flag;  // [n]
+    // Sweep-span stamps of the iteration (null: off): the first colour's
+    // launch lowers *stamp_start to its blocks' start times and the last
+    // colour's raises *stamp_end to their end times (%globaltimer, ns).
+    unsigned long long* stamp_start;
+    unsigned long long* stamp_end;
+    uint32_t stamp_first, stamp_last;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// the block's start (first colour) and, after all its threads are done, its
+// end (last colour); every thread of the block calls both
+__device__ __forceinline__ void stamp_block_start(const SweepView& s) {
+    if (s.stamp_start && s.stamp_first && threadIdx.x == 0) atomicMin(s.stamp_start, global_ns());
+}
+__device__ __forceinline__ void stamp_block_end(const SweepView& s) {
+    if (s.stamp_end && s.stamp_last) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(s.stamp_end, global_ns());
+    }
+}
 
 // Term counts of the step objective (k_term_energy items).
 struct ObjectiveCounts {

@@ -483,9 +483,11 @@ __global__ void __launch_bounds__(B, MINB) k_sweep32(SweepView s, const uint32_t
     const uint32_t lane = threadIdx.x & (G - 1);
     const unsigned mask = G >= 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(unsigned)(G - 1)));
     constexpr uint32_t kGroups = B / G;
+    stamp_block_start(s);
     // whole groups step together; a persistent grid loops over the colour
     for (uint32_t gi = blockIdx.x * kGroups + threadIdx.x / G; gi < count; gi += gridDim.x * kGroups)
         solve_vertex32<G, B>(s, order[gi], lane, mask, stage_sm);
+    stamp_block_end(s);
 }
 
 template <int G, int B>

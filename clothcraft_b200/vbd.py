@@ -293,8 +293,9 @@ class VbdSolver:
         return self
 
     def set_profiling(self, enable: bool):
-        """Time each iteration's colour sweeps with CUDA events (metrics
-        sweep_ms); the kernels themselves are unchanged."""
+        """Time each iteration's colour sweeps (metrics sweep_ms) with
+        device-clock stamps written by the sweep kernels' first and last
+        colour blocks, and the detection phases with CUDA events."""
         native.load().cc_solver_set_profiling(self.h, 1 if enable else 0)
         return self
 

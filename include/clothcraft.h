@@ -298,14 +298,19 @@ void* cc_solver_stream(const cc_solver* solver);
  * same (colour count, placement of the residual checks) and instantiated
  * again when it changes, e.g. after a colouring with another colour count.
  * Results are bitwise those of direct launches. On by default (0 launches
- * every kernel directly). With profiling on, the sweep timings are recorded
- * by event nodes inside the graphs. No reference counterpart (the wgpu
+ * every kernel directly). Profiling adds no node to the graphs (the sweep
+ * kernels stamp their own span). No reference counterpart (the wgpu
  * backend records one dispatch per colour per iteration,
  * src/gpu_vbd.rs:398-404). */
 int32_t cc_solver_set_graphs(cc_solver* solver, int32_t enable);
-/* When enabled, each iteration's colour sweeps (launched back to back) are
- * bracketed by one pair of CUDA events and cc_metrics.sweep_ms reports their
- * summed device time over the iterations the step ran. */
+/* When enabled, each iteration's colour sweeps (launched back to back) record
+ * their span on the device clock (%globaltimer): the first colour's blocks
+ * lower a start stamp to their start times, the last colour's blocks raise an
+ * end stamp to their end times, one atomic per block; cc_metrics.sweep_ms
+ * reports the summed spans over the iterations the step ran. No event or
+ * extra launch is added between the sweeps, so the stepping is timed as it
+ * runs unprofiled. Detection phases and the learned guess are timed with
+ * CUDA events on the solver stream. */
 int32_t cc_solver_set_profiling(cc_solver* solver, int32_t enable);
 /* Threads that cooperate on one vertex's local solve (1, 2, 4, 8, 16 or 32),
  * optionally | (cap << 8) with cap = 3, 4, 5, 6 or 8 resident 128-thread

@@ -6,8 +6,10 @@ membrane and bending derivatives in FP32, so its iterates are not the CPU
 path's bits; the bars are the contract's tolerances instead:
   (a) per-vertex positions after one step within 1e-5 m (fixed iteration
       counts, so both sides run the same number of sweeps);
-  (b) energy and residuals within 1 % after 100 steps of each side's own
-      trajectory (config 0);
+  (b) energy and residual_rms_n within 1 % after 100 steps of each side's
+      own trajectory (config 0), and the relative force residual inside the
+      spread of FP64 runs from starts 1e-12..1e-8 m apart (that quantity is
+      chaotic in the trajectory);
   and on the benchmarked fold the residual target (1e-3, evaluated in FP64)
   is reached in about as many iterations as the FP64 form needs.
 """
@@ -64,14 +66,41 @@ def test_fp32_config0_step_within_1e5_m_of_oracle():
     assert mg["colors"] == mo["colors"]
 
 
+def fp64_ensemble_residuals(sc, steps, perturbations, seed=7):
+    """Relative force residual of the last step after `steps` FP64 steps from
+    the scene's start with every free vertex displaced by `eps` times a seeded
+    standard normal (one run per eps; eps = 0 is the unperturbed run)."""
+    s = sc.settings
+    s.residual_check_every = s.iterations
+    s.sweep_precision = 0
+    st = s.to_c()
+    free = sc.mesh.pinned[:, None] == 0
+    out = []
+    for eps in perturbations:
+        rng = np.random.default_rng(seed)
+        x = sc.x0 + eps * rng.standard_normal(sc.x0.shape) * free
+        v, t = sc.v0.copy(), 0.0
+        g = VbdSolver(sc)
+        for _ in range(steps):
+            x, v, t, m = g.step(x, v, t, st)
+        out.append(m["relative_force_residual"])
+    return out
+
+
 def test_fp32_config0_hundred_steps_energy_and_residual():
-    """Bar (b) for the FP32 form, measured: after 100 steps of each side's own
+    """Bar (b) for the FP32 form: after 100 steps of each side's own
     trajectory the potential energy and the reference's residual_rms_n agree
-    within 1 %, but the relative force residual of the 20-iteration step does
-    not (measured 0.0592 against the FP64 path's 0.0680, 13 %): the FP32
-    trajectory has drifted from the FP64 one by then, and an unconverged
-    step's residual follows the state closely. This is the evidence that the
-    parity form stays FP64; the test pins the measured gap (within 25 %)."""
+    with the FP64 CPU path within 1 %.
+
+    The relative force residual of a 20-iteration step is not a quantity two
+    trajectories can agree on to 1 % unless they are the same to the last
+    bits: the sheet's contact with the sphere makes the trajectory chaotic, so
+    FP64 runs whose starts differ by 1e-12 m end 100 steps later several
+    millimetres apart, with relative force residuals from 0.005 to 0.1
+    (measured on a B200: 0.068, 0.067, 0.0046 and 0.097 for displacements of
+    0, 1e-12, 1e-10 and 1e-8 m), while the FP32 run gave 0.059. The test
+    therefore pins that spread and checks that the FP32 value lies inside the
+    range of the FP64 runs (widened by 25 %)."""
     sc = scenes.config0()
     s = sc.settings
     s.residual_check_every = s.iterations
@@ -86,9 +115,6 @@ def test_fp32_config0_hundred_steps_energy_and_residual():
         xo, vo, to, mo = o.step(xo, vo, to, st64)
     assert mo["contact_terms"] > 0
     assert abs(mg["residual_rms_n"] - mo["residual_rms_n"]) <= RELATIVE_TOL * abs(mo["residual_rms_n"])
-    for key in ("relative_force_residual", "relative_residual"):
-        print("%s after 100 steps: fp32 %.4g fp64 oracle %.4g" % (key, mg[key], mo[key]))
-        assert abs(mg[key] - mo[key]) <= 0.25 * abs(mo[key]), (key, mg[key], mo[key])
     grav = np.array(st64.gravity)
 
     def potential(x):
@@ -97,6 +123,13 @@ def test_fp32_config0_hundred_steps_energy_and_residual():
 
     eg, eo = potential(xg), potential(xo)
     assert abs(eg - eo) <= RELATIVE_TOL * abs(eo), (eg, eo)
+    # the spread of the FP64 path itself under starts 1e-12..1e-8 m apart
+    ens = fp64_ensemble_residuals(scenes.config0(), 100, (0.0, 1e-12, 1e-10, 1e-8))
+    print("relative force residual after 100 steps: fp32 %.4g, fp64 oracle %.4g, fp64 ensemble %s" % (
+        mg["relative_force_residual"], mo["relative_force_residual"], ["%.4g" % r for r in ens]))
+    assert abs(ens[0] - mo["relative_force_residual"]) <= RELATIVE_TOL * mo["relative_force_residual"]
+    assert max(ens) > 1.1 * min(ens), ens  # the quantity does not survive a 1e-12 m change of the start
+    assert 0.8 * min(ens) <= mg["relative_force_residual"] <= 1.25 * max(ens), (mg["relative_force_residual"], ens)
 
 
 def fold_state():
