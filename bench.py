@@ -274,6 +274,60 @@ def batched_leg(rank, world, leg, L):
             "timing": "CUDA events on the solver stream, max over ranks; replicas shard the instances"}
 
 
+CRUMPLE_WARMUP = 30   # untimed steps from the flat start (the corners travel 0.1 m), the first autotunes
+CRUMPLE_STEPS = 4
+
+
+def crumple_leg(rank, world, max_over_ranks):
+    """Config 4: the 1024x1024 sheet (1,048,576 vertices, 2,093,058 triangles)
+    with its corners pinned and driven inward at 0.2 m/s, radius 0.5 mm, 40
+    iterations. The caller moves the pinned rows between steps, so each step
+    goes through host arrays (VbdSolver.step: x and v copied in and out); after
+    CRUMPLE_WARMUP untimed steps, CRUMPLE_STEPS steps are timed by the host
+    clock around the blocking step calls (the corner update outside it), each
+    with one FP64 relative-residual evaluation after its last iteration. Every
+    rank steps its own replica; the time is the maximum over ranks."""
+    from clothcraft_b200 import scenes
+    from clothcraft_b200.vbd import VbdSolver
+
+    sc = scenes.config4()
+    t0 = time.perf_counter()
+    g = VbdSolver(sc)
+    create_s = time.perf_counter() - t0
+    s = sc.settings
+    x, v, t = sc.x0.copy(), sc.v0.copy(), 0.0
+    s.residual_check_every = 0
+    st = s.to_c()
+    for _ in range(CRUMPLE_WARMUP):
+        x = scenes.driven_corners(sc, x, t + s.dt)
+        x, v, t, _ = g.step(x, v, t, st)
+    s.residual_check_every = s.iterations
+    st = s.to_c()
+    wall, mets = 0.0, []
+    for _ in range(CRUMPLE_STEPS):
+        x = scenes.driven_corners(sc, x, t + s.dt)
+        h0 = time.perf_counter()
+        x, v, t, m = g.step(x, v, t, st)
+        wall += time.perf_counter() - h0
+        mets.append(m)
+    ms = max_over_ranks(1000.0 * wall)
+    free = int((sc.mesh.pinned == 0).sum())
+    return {"workload": "config 4: 1024x1024 sheet (%d vertices, %d triangles), 1 m, corners driven inward at "
+                        "0.2 m/s, OGC r 0.5 mm, 40 iterations; timed steps %d..%d from the flat start"
+                        % (sc.n, len(sc.mesh.triangles), CRUMPLE_WARMUP, CRUMPLE_WARMUP + CRUMPLE_STEPS - 1),
+            "steps": CRUMPLE_STEPS, "steps_per_s": world * CRUMPLE_STEPS / (ms / 1000.0),
+            "ms_per_step": ms / CRUMPLE_STEPS,
+            "vertex_iters_per_s": world * free * sum(int(m["iterations"]) for m in mets) / (ms / 1000.0),
+            "detection_ms_per_step": float(np.mean([m["detection_ms"] for m in mets])),
+            "detections_per_step": float(np.mean([m["detection_updates"] for m in mets])),
+            "contact_terms_last": int(mets[-1]["contact_terms"]),
+            "relative_force_residuals": [None if m["relative_force_residual"] is None
+                                         else float(m["relative_force_residual"]) for m in mets],
+            "solver_create_s": create_s,
+            "timing": "host clock around each blocking VbdSolver.step on host arrays (x, v in and out), max over "
+                      "ranks; replicas"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
@@ -312,6 +366,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances (config 2) leg")
+    ap.add_argument("--no-crumple", action="store_true", help="skip the 1024x1024 crumple (config 4) leg")
     ap.add_argument("--lanes", type=int, default=0,
                     help="lanes per vertex solve (1..32); 0 = autotune on the first step")
     args = ap.parse_args()
@@ -524,6 +579,9 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_leg(rank, world, leg, L)
+    crumple = None
+    if not args.no_crumple:
+        crumple = crumple_leg(rank, world, max_over_ranks)
 
     # ---- CPU baseline (rank 0, N=1 only): the oracle at equal residual from
     # the state the timed legs start from, a sample of about 30 s
@@ -617,6 +675,7 @@ def main():
         "detections_per_step": sum(m["detection_updates"] for m in mets_l) / K,
         "contact_terms_last": mets_l[-1]["contact_terms"] if mets_l else None,
         "batched": batched,
+        "crumple": crumple,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -61,6 +61,26 @@ def test_forward_tensor_cores_matches_oracle(n):
     assert err <= TC_RTOL * scale, err
 
 
+def test_kernels_run_after_the_device_is_selected_again():
+    """The MLP kernels raise their dynamic shared-memory limit on the device
+    current at each launch (the limit is a per-device attribute): after
+    cc_set_device selects the device again, tcgen05 and FP32 inference still
+    run and match the oracle."""
+    from clothcraft_b200 import native
+
+    L = native.load()
+    m, p = random_net(3)
+    f = np.random.default_rng(5).standard_normal((777, 24)).astype(np.float32)
+    ref = oracle.mlp_forward(p, f)
+    scale = max(1.0, np.abs(ref).max())
+    for _ in range(2):
+        assert L.cc_set_device(torch.cuda.current_device()) == 0
+        tc = m.forward(cuda(f), precision=1).cpu().numpy()
+        f32 = m.forward(cuda(f), precision=0).cpu().numpy()
+        assert np.abs(tc - ref).max() <= TC_RTOL * scale
+        assert np.abs(f32 - ref).max() <= FP32_RTOL * scale
+
+
 def test_gradients_match_oracle():
     m, p = random_net(3)
     rng = np.random.default_rng(7)
