@@ -321,8 +321,13 @@ def crumple_leg(rank, world, max_over_ranks):
             "detection_ms_per_step": float(np.mean([m["detection_ms"] for m in mets])),
             "detections_per_step": float(np.mean([m["detection_updates"] for m in mets])),
             "contact_terms_last": int(mets[-1]["contact_terms"]),
+            "relative_residuals": [None if m["relative_residual"] is None else float(m["relative_residual"])
+                                   for m in mets],
             "relative_force_residuals": [None if m["relative_force_residual"] is None
                                          else float(m["relative_force_residual"]) for m in mets],
+            "residual_note": "relative_residuals: the KKT residual of the step's OGC-ball-constrained problem; "
+                             "relative_force_residuals: the unprojected force norm, which keeps the outward "
+                             "forces on vertices held at their ball boundaries (next to the driven corners)",
             "solver_create_s": create_s,
             "timing": "host clock around each blocking VbdSolver.step on host arrays (x, v in and out), max over "
                       "ranks; replicas"}
