@@ -36,6 +36,9 @@ __device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uin
     Sym H;
     sym_zero(H);
     double e_el = local_part<true, G>(s, v, x, lane, g, H);
+    // the OGC ball, loaded here so that its latency hides behind the reductions
+    const d3 ctr = ld3(s.contacts.centers, v);
+    const double rad = s.contacts.radii[v];
     if (G > 1) {
         e_el = group_sum<G>(e_el, mask);
         g.x = group_sum<G>(g.x, mask);
@@ -66,8 +69,16 @@ __device__ __forceinline__ void solve_vertex(const SweepView& s, uint32_t v, uin
     for (int attempt = 0; attempt < 10; ++attempt) {
         d3 cand = x + delta * scale;
         scale *= 0.5;
-        bool bound;
-        cand = truncate_ball(s, v, cand, bound);
+        // ContactSet::truncate (src/ogc/world.rs:91-100) with the loaded ball
+        bool bound = false;
+        {
+            d3 d = cand - ctr;
+            double l = len(d);
+            if (l > rad) {
+                bound = true;
+                cand = ctr + d * (rad / l);
+            }
+        }
         truncated = truncated || bound;
         d3 gd;
         Sym Hd;

@@ -111,6 +111,11 @@ __device__ __forceinline__ TriRec tri_rec(const SweepView& s, uint32_t t, uint32
 
 // axial (src/energy.rs:10-16) with its first and second derivative, FP32
 __device__ __forceinline__ void axial3f(float sv, float k, float c, float delta, float& f1, float& f2) {
+    if (c == 1.f) {  // pure quadratic law: the (1 - c) terms are exactly zero
+        f1 = k * (c * sv);
+        f2 = k * c;
+        return;
+    }
     float r = sqrtf(sv * sv + delta * delta);
     float ir = 1.f / r;
     float p = (sv + r - delta) * 0.5f;

@@ -38,8 +38,17 @@ __device__ __forceinline__ void sym_add_diag(Sym& h, double s) {
 }
 
 // ----------------------------------------------------------------- terms
-// axial (src/energy.rs:10-16) with its first and second derivative.
+// axial (src/energy.rs:10-16) with its first and second derivative. With
+// c == 1 (the pure quadratic law, e.g. StVK mapped with compression ratio 1)
+// every (1 - c) term is exactly zero, so the square root and the reciprocal
+// of the compression branch are skipped; the results are the same bits.
 __device__ __forceinline__ void axial3(double s, double k, double c, double delta, double& f, double& f1, double& f2) {
+    if (c == 1.0) {
+        f = 0.5 * k * (c * s * s);
+        f1 = k * (c * s);
+        f2 = k * c;
+        return;
+    }
     double r = sqrt(s * s + delta * delta);
     double ir = 1.0 / r;
     double p = (s + r - delta) * 0.5;
@@ -50,6 +59,7 @@ __device__ __forceinline__ void axial3(double s, double k, double c, double delt
     f2 = k * (c + (1.0 - c) * (p1 * p1 + p * p2));
 }
 __device__ __forceinline__ double axial1(double s, double k, double c, double delta) {
+    if (c == 1.0) return 0.5 * k * (c * s * s);
     double r = sqrt(s * s + delta * delta);
     double p = (s + r - delta) * 0.5;
     return 0.5 * k * (c * s * s + (1.0 - c) * p * p);
