@@ -274,6 +274,52 @@ def batched_leg(rank, world, leg, L):
             "timing": "CUDA events on the solver stream, max over ranks; replicas shard the instances"}
 
 
+GARMENT_WARMUP = 3
+GARMENT_STEPS = 5
+
+
+def garment_leg(rank, world, leg, L):
+    """Config 3's scene: two seeded 0.6 x 0.7 m panels (~20k vertices each,
+    Poisson-disk sampling and Delaunay triangulation) 5 cm either side of a
+    fixed capsule, joined along the sides and shoulders by 1e3 N/m penalty
+    stitches, contact radius 1 mm. The adaptive (plain) initial guess: the
+    learned form needs a network trained on this scene, which is not shipped.
+    Two settings from the same state: the config's fixed 20 iterations, and
+    the equal-residual form of the headline legs (1e-3 relative residual,
+    checked every 2, cap 200, stall refresh 2, Chebyshev rho 0.95).
+    GARMENT_WARMUP untimed steps, then GARMENT_STEPS device-timed steps each."""
+    from clothcraft_b200 import scenes
+    from clothcraft_b200.vbd import VbdSolver
+
+    sc = scenes.config3()
+    out = {"workload": "config 3 scene: two Poisson-disk panels (%d vertices, %d triangles) around a capsule, "
+                       "side and shoulder stitches 1e3 N/m, contact r 1 mm, adaptive initial guess"
+                       % (sc.n, len(sc.mesh.triangles))}
+    free = int((sc.mesh.pinned == 0).sum())
+    for name, target in (("fixed_20_iterations", False), ("residual_1e-3", True)):
+        s = sc.settings
+        s.init_mode = 0
+        if target:
+            s.iterations, s.residual_tolerance, s.residual_check_every = ITERATION_CAP, TOLERANCE, CHECK_EVERY
+            s.stall_refresh, s.acceleration = STALL_REFRESH, ACCELERATION
+        else:
+            s.iterations, s.residual_tolerance, s.residual_check_every = 20, 0.0, 20
+            s.stall_refresh, s.acceleration = 0, 0.0
+        st = s.to_c()
+        g = VbdSolver(sc)
+        g.set_state(sc.x0, sc.v0, 0.0)
+        for _ in range(GARMENT_WARMUP):
+            g.step_resident(st)
+        ms, mets = leg(g, lambda: g.step_resident(st), GARMENT_STEPS)
+        its = [int(m["iterations"]) for m in mets]
+        out[name] = {"steps_per_s": world * GARMENT_STEPS / (ms / 1000.0), "ms_per_step": ms / GARMENT_STEPS,
+                     "vertex_iters_per_s": world * free * sum(its) / (ms / 1000.0),
+                     "mean_iterations": float(np.mean(its)),
+                     "mean_final_relative_residual": float(np.mean([m["relative_residual"] for m in mets]))}
+    out["timing"] = "CUDA events on the solver stream, max over ranks; replicas"
+    return out
+
+
 CRUMPLE_WARMUP = 30   # untimed steps from the flat start (the corners travel 0.1 m), the first autotunes
 CRUMPLE_STEPS = 4
 
@@ -320,6 +366,8 @@ def crumple_leg(rank, world, max_over_ranks):
             "vertex_iters_per_s": world * free * sum(int(m["iterations"]) for m in mets) / (ms / 1000.0),
             "detection_ms_per_step": float(np.mean([m["detection_ms"] for m in mets])),
             "detections_per_step": float(np.mean([m["detection_updates"] for m in mets])),
+            "coloring_ms_per_step": float(np.mean([m["color_ms"] for m in mets])),
+            "coloring_rounds_per_step": float(np.mean([m["color_rounds"] for m in mets])),
             "contact_terms_last": int(mets[-1]["contact_terms"]),
             "relative_residuals": [None if m["relative_residual"] is None else float(m["relative_residual"])
                                    for m in mets],
@@ -372,6 +420,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-instances (config 2) leg")
     ap.add_argument("--no-crumple", action="store_true", help="skip the 1024x1024 crumple (config 4) leg")
+    ap.add_argument("--no-garment", action="store_true", help="skip the garment-proxy (config 3) leg")
     ap.add_argument("--lanes", type=int, default=0,
                     help="lanes per vertex solve (1..32); 0 = autotune on the first step")
     args = ap.parse_args()
@@ -584,6 +633,9 @@ def main():
     batched = None
     if not args.no_batched:
         batched = batched_leg(rank, world, leg, L)
+    garment = None
+    if not args.no_garment:
+        garment = garment_leg(rank, world, leg, L)
     crumple = None
     if not args.no_crumple:
         crumple = crumple_leg(rank, world, max_over_ranks)
@@ -680,6 +732,7 @@ def main():
         "detections_per_step": sum(m["detection_updates"] for m in mets_l) / K,
         "contact_terms_last": mets_l[-1]["contact_terms"] if mets_l else None,
         "batched": batched,
+        "garment": garment,
         "crumple": crumple,
     }
     print(json.dumps(line), flush=True)
