@@ -21,6 +21,12 @@ iteration), and so does the reference's fixed 30-iteration step
 (`fixed_iterations`). The network is clothcraft_b200/data/fold_init_mlp.npz,
 trained by `python -m clothcraft_b200.train_init fold` on other seeds.
 
+Further keys time the other configurations on the same box: `batched` (96
+uneven instances in one solver, ~3.66M vertices, 20 iterations), `garment`
+(the sewn two-panel scene at 20 iterations and at the 1e-3 target) and
+`crumple` (the 1024x1024 sheet with driven corners, 40 iterations, host
+arrays); --no-batched / --no-garment / --no-crumple skip them.
+
   python bench.py [--gpus N --steps K --warmup W]      # B200 library
   python bench.py --impl reference [...]                # CPU path (oracle restatement)
 
