@@ -393,7 +393,9 @@ def run_reference(args, rank, world):
         return 0
     sc = workload()
     threads = os.cpu_count() or 1
-    budget = float(os.environ.get("CC_REFERENCE_BUDGET_S", "480"))
+    # timed part bounded so that warm-up and timed steps end within a few minutes
+    # (the oracle takes ~8-11 s a fold step on 16 host threads)
+    budget = float(os.environ.get("CC_REFERENCE_BUDGET_S", "200"))
     warm_budget = float(os.environ.get("CC_REFERENCE_WARMUP_BUDGET_S", "45"))
     done, dt, (its, force), warm = cpu_reference_run(sc, fold_state(), args.steps, budget, threads,
                                                      warmup=args.warmup, warmup_budget_s=warm_budget)
