@@ -516,7 +516,8 @@ struct cc_solver {
             if (e) cudaEventDestroy(e);
         if (learn0) cudaEventDestroy(learn0);
         if (learn1) cudaEventDestroy(learn1);
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        for (auto& e : graph_cache)
+            if (e.second) cudaGraphExecDestroy(e.second);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -596,32 +597,55 @@ struct cc_solver {
 
     // CUDA-graph launch of the iteration chunks (cc_solver_set_graphs)
     bool graphs = true;
-    cudaGraphExec_t graph_exec = nullptr;
+    // executable graphs by shape (node count): a batch's lead chunk and the
+    // full chunks after it have different shapes, and each keeps its own
+    // executable, updated in place while its shape holds
+    std::vector<std::pair<size_t, cudaGraphExec_t>> graph_cache;
+    static constexpr size_t kGraphCacheSize = 6;
     uint64_t graph_instantiations = 0, graph_updates = 0;
     void launch_captured_chunk() {
         cudaGraph_t g = nullptr;
         CC_CUDA(cudaStreamEndCapture(stream, &g));
-        if (graph_exec) {
+        size_t nodes = 0;
+        cudaError_t ce = cudaGraphGetNodes(g, nullptr, &nodes);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(g);
+            cuda_check(ce, "cudaGraphGetNodes");
+        }
+        cudaGraphExec_t* slot = nullptr;
+        for (auto& e : graph_cache)
+            if (e.first == nodes) slot = &e.second;
+        bool updated = false;
+        if (slot && *slot) {
             cudaGraphExecUpdateResultInfo info;
-            if (cudaGraphExecUpdate(graph_exec, g, &info) == cudaSuccess) {
+            if (cudaGraphExecUpdate(*slot, g, &info) == cudaSuccess) {
                 ++graph_updates;
+                updated = true;
             } else {
-                (void)cudaGetLastError();  // a topology change: not an error
-                cudaGraphExecDestroy(graph_exec);
-                graph_exec = nullptr;
+                (void)cudaGetLastError();  // another topology with the same node count: not an error
+                cudaGraphExecDestroy(*slot);
+                *slot = nullptr;
             }
         }
-        if (!graph_exec) {
-            cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+        if (!updated) {
+            if (!slot) {
+                if (graph_cache.size() >= kGraphCacheSize) {  // drop the oldest shape
+                    if (graph_cache.front().second) cudaGraphExecDestroy(graph_cache.front().second);
+                    graph_cache.erase(graph_cache.begin());
+                }
+                graph_cache.push_back({nodes, nullptr});
+                slot = &graph_cache.back().second;
+            }
+            cudaError_t e = cudaGraphInstantiate(slot, g, 0);
             if (e != cudaSuccess) {
                 cudaGraphDestroy(g);
-                graph_exec = nullptr;
+                *slot = nullptr;
                 cuda_check(e, "cudaGraphInstantiate");
             }
             ++graph_instantiations;
         }
         CC_CUDA(cudaGraphDestroy(g));
-        CC_CUDA(cudaGraphLaunch(graph_exec, stream));
+        CC_CUDA(cudaGraphLaunch(*slot, stream));
     }
     void step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* out);
     void autotune(const SweepView& sv, bool fp32);
@@ -936,16 +960,25 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
         }
         const uint32_t chunk = target_on ? std::max<uint32_t>(check_every, 4) : s.iterations;
         uint32_t chunks = 0;
-        // graph mode: each chunk's launches are captured into a CUDA graph; the
-        // executable graph is updated in place while the chunk's topology (the
-        // colour count and the placement of the residual checks) stays the
-        // same, and instantiated anew when it changes
+        // graph mode: each chunk's launches (after a batch's first iteration)
+        // are captured into a CUDA graph; the executable graph of the chunk's
+        // shape is updated in place, and a new shape (another colour count or
+        // placement of the residual checks) is instantiated once and kept
         const bool capture = graphs;
         for (uint32_t c0 = it0; c0 < s.iterations; c0 += chunk) {
             uint32_t c1 = std::min(s.iterations, c0 + chunk);
-            if (capture) CC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+            // the batch's first iteration goes out as direct launches: the GPU
+            // starts on it while the host captures the rest of the lead chunk
+            // (the capture and the executable-graph update of the first chunk
+            // after a detection would otherwise leave the GPU idle)
+            const uint32_t cap_from = (capture && c0 == it0) ? c0 + 1 : c0;
+            bool capturing = false;
             try {
             for (uint32_t it = c0; it < c1; ++it) {
+                if (capture && it == cap_from) {
+                    CC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+                    capturing = true;
+                }
                 sv.iteration = it;
                 sv.clipped = &sc.ptr->clipped_iter[it];
                 // profiling: the iteration's back-to-back colour sweeps stamp
@@ -977,14 +1010,14 @@ void cc_solver::step(const cc_vbd_settings& s, const cc_grab* grab, cc_metrics* 
                 }
             }
             } catch (...) {
-                if (capture) {  // leave the stream out of capture mode before the failure propagates
+                if (capturing) {  // leave the stream out of capture mode before the failure propagates
                     cudaGraph_t g = nullptr;
                     cudaStreamEndCapture(stream, &g);
                     if (g) cudaGraphDestroy(g);
                 }
                 throw;
             }
-            if (capture) launch_captured_chunk();
+            if (capturing) launch_captured_chunk();
             CC_CUDA(cudaGetLastError());
             if (c1 >= s.iterations || !target_on) break;
             // look ahead: enqueue the next chunk before waiting on this one's stop flag

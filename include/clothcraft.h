@@ -293,10 +293,11 @@ uint64_t cc_solver_total(const cc_solver* solver);
 void* cc_solver_stream(const cc_solver* solver);
 /* When enabled, each chunk of iterations the step enqueues ahead of the
  * device (all iterations without a residual target; max(check_every, 4)
- * with one) is captured into a CUDA graph and launched as one; the
- * executable graph is updated in place while the chunk's topology stays the
- * same (colour count, placement of the residual checks) and instantiated
- * again when it changes, e.g. after a colouring with another colour count.
+ * with one) is captured into a CUDA graph and launched as one, except the
+ * first iteration after each detection, which is launched directly so that
+ * the device works while the rest of its chunk is captured. Executable
+ * graphs are kept per chunk shape (colour count, placement of the residual
+ * checks) and updated in place while the shape recurs.
  * Results are bitwise those of direct launches. On by default (0 launches
  * every kernel directly). Profiling adds no node to the graphs (the sweep
  * kernels stamp their own span). No reference counterpart (the wgpu
